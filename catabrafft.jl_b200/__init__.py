@@ -1,0 +1,254 @@
+"""B200-native 1D complex FFT behind CatabraFFT.jl's public API.
+
+Python mirror of the reference's API (src/CatabraFFT.jl), dispatching every
+transform to libcatabra_b200.so (CUDA, sm_100a) through its C ABI:
+
+    fft(x)            CatabraFFT.jl:65-72    forward, allocates the result
+    ifft(x)           CatabraFFT.jl:88-101   inverse, scaled by 1/n
+    bfft(x)           CatabraFFT.jl:103-115  inverse, unscaled
+    fft_(x)           CatabraFFT.jl:46-49    in place (Julia's fft!)
+    plan_fft(x, flag) CatabraFFT.jl:149-167  returns a Spell
+    p * x, mul_(y,p,x) CatabraFFT.jl:186-196
+    empty_cache()     CatabraFFT.jl:39-43
+    NO_FLAG, MEASURE, ENCHANT                spells.jl:4-8
+
+``x`` is a complex128 (ComplexF64) or complex64 (ComplexF32) array whose last
+axis is transformed: 1-D of length n, or 2-D [batch, n] for a batch of
+transforms.  numpy arrays (and CPU torch tensors) go through the host entry
+point (copy in, transform, copy out); CUDA torch tensors stay on the device
+and run on torch's current stream.  Inputs are never modified, except by
+``fft_``.  Errors raise :class:`CatabraError` (a RuntimeError) or
+ValueError/TypeError for arguments the reference would also reject.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BACKWARD, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERSE, MEASURE,
+                   NO_FLAG, CatabraError, check)
+
+FLAG = int
+PLANNER_DEFAULT = NO_FLAG
+
+__all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache",
+           "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
+           "describe_strategy", "version"]
+
+_cache_lock = threading.Lock()
+_plans: dict = {}
+
+
+def version() -> int:
+    return _lib.LIB.cfft_version()
+
+
+def describe_strategy(n: int, dtype=np.complex128) -> str:
+    """The planner's choice for length n (host logic only, no device work)."""
+    buf = ctypes.create_string_buffer(512)
+    check(_lib.LIB.cfft_describe_strategy(int(n), _dtype_code(dtype), buf, 512))
+    return buf.value.decode()
+
+
+def _dtype_code(dt) -> int:
+    name = str(dt).replace("torch.", "")
+    if name in ("complex128", "<class 'numpy.complex128'>"):
+        return C128
+    if name in ("complex64", "<class 'numpy.complex64'>"):
+        return C64
+    raise TypeError(f"unsupported element type {dt}: expected complex128 or complex64")
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+class _Plan:
+    """Owns one cfft_plan handle (device tables, scratch)."""
+
+    def __init__(self, n, batch, dtype, flags, device):
+        self.n, self.batch, self.dtype, self.flags, self.device = n, batch, dtype, flags, device
+        h = ctypes.c_void_p()
+        check(_lib.LIB.cfft_plan_create(ctypes.byref(h), n, batch, dtype, flags))
+        self.handle = h
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        check(_lib.LIB.cfft_plan_describe(self.handle, buf, 512))
+        return buf.value.decode()
+
+    def launches(self) -> int:
+        return _lib.LIB.cfft_plan_launches(self.handle)
+
+    def workspace_bytes(self) -> int:
+        return _lib.LIB.cfft_plan_workspace_bytes(self.handle)
+
+    def destroy(self):
+        if self.handle:
+            _lib.LIB.cfft_plan_destroy(self.handle)
+            self.handle = None
+
+
+def _current_device(x=None) -> int:
+    if x is not None and _is_torch(x) and x.is_cuda:
+        return x.device.index
+    return 0
+
+
+def _get_plan(n, batch, dtype, flags, device) -> _Plan:
+    key = (device, n, batch, dtype, flags)
+    with _cache_lock:
+        p = _plans.get(key)
+        if p is None:
+            p = _Plan(n, batch, dtype, flags, device)
+            _plans[key] = p
+        return p
+
+
+def _shape(x):
+    if x.ndim == 1:
+        return x.shape[0], 1
+    if x.ndim == 2:
+        return x.shape[1], x.shape[0]
+    raise ValueError("expected a vector of length n or a [batch, n] matrix")
+
+
+def _run(x, direction: int, flags: int = NO_FLAG, out=None):
+    if _is_torch(x):
+        import torch
+        if x.is_cuda:
+            n, batch = _shape(x)
+            if n < 1:
+                raise ValueError("transform length must be >= 1")
+            dt = _dtype_code(x.dtype)
+            xc = x.contiguous()
+            y = torch.empty_like(xc) if out is None else out
+            if batch == 0:
+                return y
+            plan = _get_plan(n, batch, dt, flags, x.device.index)
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+            with torch.cuda.device(x.device):
+                check(_lib.LIB.cfft_execute(plan.handle, ctypes.c_void_p(xc.data_ptr()),
+                                            ctypes.c_void_p(y.data_ptr()), direction,
+                                            ctypes.c_void_p(stream)))
+            return y
+        xn = x.detach().numpy()
+        y = _run(xn, direction, flags)
+        return torch.from_numpy(y)
+    a = np.asarray(x)
+    n, batch = _shape(a)
+    if n < 1:
+        raise ValueError("transform length must be >= 1")
+    dt = _dtype_code(a.dtype)
+    a = np.ascontiguousarray(a)
+    y = np.empty_like(a) if out is None else out
+    if batch == 0:
+        return y
+    plan = _get_plan(n, batch, dt, flags, 0)
+    check(_lib.LIB.cfft_execute_host(plan.handle, a.ctypes.data_as(ctypes.c_void_p),
+                                     y.ctypes.data_as(ctypes.c_void_p), direction))
+    return y
+
+
+def fft(x):
+    """Forward DFT along the last axis (CatabraFFT.fft)."""
+    return _run(x, FORWARD)
+
+
+def ifft(x):
+    """Inverse DFT scaled by 1/n (CatabraFFT.ifft: conj, fft, conj, /n)."""
+    return _run(x, INVERSE)
+
+
+def bfft(x):
+    """Unscaled inverse DFT (CatabraFFT.bfft)."""
+    return _run(x, BACKWARD)
+
+
+def fft_(x):
+    """In-place forward DFT (Julia's fft!); returns x."""
+    if _is_torch(x) and x.is_cuda:
+        if not x.is_contiguous():
+            raise ValueError("fft_ needs a contiguous tensor")
+        _run(x, FORWARD, out=x)
+        return x
+    if not (isinstance(x, np.ndarray) and x.flags.c_contiguous and x.flags.writeable):
+        raise ValueError("fft_ needs a writeable C-contiguous array")
+    _run(x, FORWARD, out=x)
+    return x
+
+
+class Spell:
+    """Plan object (the reference's Spell{T}, src/spells.jl:18-37).
+
+    Holds n, datatype, flag and inverse like the reference; ``p * x`` and
+    ``mul_(y, p, x)`` run the planned transform.  Unlike the reference, the
+    flag is honoured at execution (spells.jl/kernel.jl:97 always ran the
+    NO_FLAG function) and x is never overwritten.
+    """
+
+    def __init__(self, n: int, datatype, flag: int = NO_FLAG, batch: int = 1, device: int = 0):
+        if n < 1:
+            raise ValueError("transform length must be >= 1")
+        self.n = int(n)
+        self.datatype = datatype
+        self.flag = int(flag)
+        self.batch = int(batch)
+        self.inverse = None
+        self._plan = _get_plan(self.n, self.batch, _dtype_code(datatype), self.flag, device)
+
+    def describe(self) -> str:
+        return self._plan.describe()
+
+    def launches(self) -> int:
+        return self._plan.launches()
+
+    def _check(self, x):
+        n, batch = _shape(x)
+        if n != self.n or batch != self.batch:
+            raise ValueError(f"plan is for n={self.n}, batch={self.batch}; got n={n}, batch={batch}")
+
+    def __mul__(self, x):
+        self._check(x)
+        return _run(x, FORWARD, self.flag)
+
+    __matmul__ = __mul__
+
+    def __call__(self, x):
+        return fft(x)
+
+    def __repr__(self):
+        return f"Spell{{{self.datatype}}}(n={self.n}, flag={self.flag}, batch={self.batch})"
+
+
+def plan_fft(x, flags: int = NO_FLAG) -> Spell:
+    """Plan a forward FFT for arrays shaped like x (CatabraFFT.plan_fft)."""
+    if int(flags) & 3 not in (NO_FLAG, MEASURE, ENCHANT):
+        raise ValueError("flags must be NO_FLAG, MEASURE or ENCHANT")
+    n, batch = _shape(x)
+    dev = _current_device(x)
+    return Spell(n, x.dtype, flags, batch, dev)
+
+
+def mul_(y, p: Spell, x):
+    """y <- p * x (LinearAlgebra.mul! of the reference); returns y."""
+    p._check(x)
+    p._check(y)
+    if _is_torch(x) and x.is_cuda:
+        _run(x, FORWARD, p.flag, out=y)
+        return y
+    r = _run(x, FORWARD, p.flag)
+    np.copyto(y, r)
+    return y
+
+
+def empty_cache() -> None:
+    """Free every cached plan and its device memory (CatabraFFT.empty_cache)."""
+    with _cache_lock:
+        for p in _plans.values():
+            p.destroy()
+        _plans.clear()
+    check(_lib.LIB.cfft_empty_cache())

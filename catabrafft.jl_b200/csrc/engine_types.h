@@ -1,0 +1,50 @@
+// engine_types.h -- parameter blocks shared by the kernels and the planner.
+#pragma once
+#include <vector_types.h>
+
+#define CFFT_MAXP 24
+
+struct SubPlan {
+    int L;                        // sub-transform length
+    int np;                       // number of radix passes
+    int G;                        // sub-transforms per wave (fits EMAX regs/thread)
+    unsigned char radix[CFFT_MAXP];
+    const void* tw;               // w_L^m, m < L, element type of the data
+};
+
+struct TwoLevel {                 // w_N^e = lo[e & mask] * hi[e >> bits]  (FP64)
+    const double2* lo;
+    const double2* hi;
+    int bits;
+    int N;
+};
+
+enum { MODE_ROWS = 0, MODE_FOUR = 1, MODE_COLPASS = 2, MODE_ROWPASS = 3 };
+enum { CONV_NONE = 0, CONV_RADER = 1, CONV_BLUE = 2 };
+enum { PRE_NONE = 0, PRE_CHIRP = 1, PRE_SPEC = 2 };      // COLPASS prologue
+enum { POST_OUT = 0, POST_RAW = 1, POST_CHIRP = 2 };     // ROWPASS epilogue
+
+struct KParams {
+    int mode, conv;
+    int nx;                       // user transform length
+    int M;                        // working FFT length (nx unless conv)
+    int N1, N2, C;                // FOUR / pass split
+    int V;                        // ROWS: transforms per CTA; passes: tile width
+    int PA, PC;                   // smem pitches (column layout / row layout)
+    int XP;                       // Rader x staging: row pitch (ROWS) or chunk (FOUR)
+    int pre, post;                // pass prologue / epilogue
+    SubPlan pa, pc;               // column (N1) / row (N2, or M in ROWS) plans
+    TwoLevel t4;                  // four-step twiddles w_M^(i2 k1)
+    const int* perm;              // Rader: g^j mod nx, j < nx-1
+    const int* iperm;             // Rader: g^-j mod nx
+    const double2* chirp;         // Bluestein: exp(-i pi j^2 / nx), j < nx
+    const double2* spec;          // conv spectrum / M (FP64)
+    const void* in;
+    void* out;
+    long long in_dist, out_dist;  // elements between consecutive transforms
+    int batch;                    // transforms in this launch
+    int units;                    // CTAs (ROWS/FOUR clusters) or tiles per transform
+    int dir;                      // 0 forward, 1 inverse (scaled), 2 backward
+    double scale;                 // 1/nx for dir 1, else 1
+};
+

@@ -1,0 +1,922 @@
+// plan.cpp -- planner, FP64 table generation, plan cache and the C ABI.
+//
+// Host-side counterpart of CatabraFFT.jl's dispatcher (src/kernel.jl:72-199),
+// planner (src/radix_plan.jl) and plan object (src/spells.jl).  Strategy:
+//   n 7-smooth          -> Stockham on the device (ROWS / FOUR / two HBM passes)
+//   n prime             -> Rader (src/prime.jl): generator permutation, cyclic
+//                          convolution of length n-1 through a zero-padded
+//                          smooth FFT of length M >= 2n-3, inverse permutation
+//   other n             -> Bluestein convolution of length M >= 2n-1 (the
+//                          reference recurses through mixed radix + Rader,
+//                          src/kernel.jl:84-86; both compute the same DFT)
+// Tables are generated here in FP64 with exact integer angle reduction and
+// rounded once to the data type.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/catabra_b200.h"
+#include "kernels.h"
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+#define CUDA_TRY(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? CFFT_ERR_NOMEM : CFFT_ERR_CUDA,  \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+// ------------------------------------------------------------ integer helpers
+static bool is_smooth7(int64_t n) {
+    if (n < 1) return false;
+    for (int p : {2, 3, 5, 7})
+        while (n % p == 0) n /= p;
+    return n == 1;
+}
+static bool is_prime64(int64_t n) {
+    if (n < 2) return false;
+    if (n % 2 == 0) return n == 2;
+    for (int64_t d = 3; d * d <= n; d += 2)
+        if (n % d == 0) return false;
+    return true;
+}
+static int64_t smooth_ceil(int64_t n) {
+    for (int64_t m = std::max<int64_t>(n, 1);; m++)
+        if (is_smooth7(m)) return m;
+}
+static int64_t powmod(int64_t b, int64_t e, int64_t m) {
+    __int128 r = 1, x = b % m;
+    while (e > 0) {
+        if (e & 1) r = (r * x) % m;
+        x = (x * x) % m;
+        e >>= 1;
+    }
+    return (int64_t)r;
+}
+// smallest primitive root (the generator search of src/prime.jl:9-28)
+static int64_t primitive_root(int64_t p) {
+    int64_t phi = p - 1;
+    std::vector<int64_t> fac;
+    int64_t f = phi;
+    for (int64_t q = 2; q * q <= f; q++)
+        if (f % q == 0) {
+            fac.push_back(q);
+            while (f % q == 0) f /= q;
+        }
+    if (f > 1) fac.push_back(f);
+    for (int64_t g = 2; g < p; g++) {
+        bool ok = true;
+        for (int64_t q : fac)
+            if (powmod(g, phi / q, p) == 1) { ok = false; break; }
+        if (ok) return g;
+    }
+    return -1;
+}
+
+// greedy radix split, largest first (create_std_radix_plan, radix_plan.jl:100-138,
+// over the codelet set of this build)
+static const int kRadices[] = {16, 9, 8, 7, 5, 4, 3, 2};
+static std::vector<int> radix_split(int64_t L, const int* order = kRadices, int nord = 8) {
+    std::vector<int> r;
+    while (L > 1) {
+        int c = 0;
+        for (int i = 0; i < nord; i++)
+            if (L % order[i] == 0) { c = order[i]; break; }
+        if (!c) return {};
+        r.push_back(c);
+        L /= c;
+    }
+    return r;
+}
+static int wave_G(const std::vector<int>& rad, int64_t L, int T) {
+    if (L <= 1) return 1 << 20;
+    int64_t g = 1 << 20;
+    for (int r : rad) g = std::min<int64_t>(g, (int64_t)T * (CFFT_EMAX / r) * r / L);
+    return (int)g;
+}
+
+// ------------------------------------------------------------- FP64 tables
+// exp(sign * 2 pi i m / N) with exact integer reduction, long double kernel
+static double2 omega(int64_t m, int64_t N, int sign) {
+    m %= N;
+    if (m < 0) m += N;
+    // quadrant: theta = (pi/2) (q + r/N)
+    __int128 fm = (__int128)4 * m;
+    int64_t q = (int64_t)(fm / N);
+    int64_t r = (int64_t)(fm - (__int128)q * N);
+    const long double HALF_PI = 1.570796326794896619231321691639751442L;
+    long double c, s;
+    if (2 * r <= N) {
+        long double x = HALF_PI * ((long double)r / (long double)N);
+        c = cosl(x);
+        s = sinl(x);
+    } else {
+        long double x = HALF_PI * ((long double)(N - r) / (long double)N);
+        c = sinl(x);
+        s = cosl(x);
+    }
+    long double cc, ss;
+    switch (q & 3) {
+        case 0: cc = c; ss = s; break;
+        case 1: cc = -s; ss = c; break;
+        case 2: cc = -c; ss = -s; break;
+        default: cc = s; ss = -c; break;
+    }
+    return make_double2((double)cc, (double)(sign * ss));
+}
+// Julia's robust complex inverse (Smith's algorithm) for |z| near 1
+static double2 julia_inv(double2 z) {
+    volatile double c = z.x, d = z.y;
+    double p, q;
+    if (std::fabs(c) >= std::fabs(d)) {
+        volatile double r = d / c;
+        volatile double den = c + d * r;
+        volatile double t = 1.0 / den;
+        p = t;
+        q = -r * t;
+    } else {
+        volatile double cc = d, dd = c;
+        volatile double r = dd / cc;
+        volatile double den = cc + dd * r;
+        volatile double t = 1.0 / den;
+        p = r * t;
+        q = -t;
+    }
+    return make_double2(p, q);
+}
+static double2 cmul_h(double2 a, double2 b) {
+    volatile double re1 = a.x * b.x, re2 = a.y * b.y, im1 = a.x * b.y, im2 = a.y * b.x;
+    return make_double2(re1 - re2, im1 + im2);
+}
+// power_by_squaring (Julia Base) -- the reference builds Rader twiddles with it
+static double2 pow_by_squaring(double2 x, int64_t p) {
+    if (p == 1) return x;
+    if (p == 0) return make_double2(1, 0);
+    if (p == 2) return cmul_h(x, x);
+    int t = __builtin_ctzll((unsigned long long)p) + 1;
+    p >>= t;
+    while ((t -= 1) > 0) x = cmul_h(x, x);
+    double2 y = x;
+    while (p > 0) {
+        t = __builtin_ctzll((unsigned long long)p) + 1;
+        p >>= t;
+        while ((t -= 1) >= 0) x = cmul_h(x, x);
+        y = cmul_h(y, x);
+    }
+    return y;
+}
+
+// ---------------------------------------------------------------- plan state
+struct Stage {
+    KParams kp;
+    unsigned grid;
+    int threads;
+    size_t smem;
+    int cluster;
+    int in_sel, out_sel;     // 0 user in, 1 user out, 2 scratch0, 3 scratch1
+};
+
+struct Shape {
+    int mode = MODE_ROWS;    // ROWS, FOUR or GLOBAL(=MODE_COLPASS)
+    int conv = CONV_NONE;
+    int64_t M = 0;
+    int N1 = 1, N2 = 1, C = 1, V = 1;
+    std::vector<int> ra, rc; // radix passes for N1 / N2 (ROWS: rc for M)
+    size_t smem = 0;
+    double score = 0;
+};
+
+struct cfft_plan_s {
+    int64_t n = 0, batch = 0;
+    int dtype = 0, flags = 0;
+    Shape shape;
+    std::string desc;
+    std::vector<Stage> stages;
+    int64_t chunk = 0;       // transforms per stage sequence (GLOBAL)
+    void* scratch[2] = {nullptr, nullptr};
+    size_t scratch_bytes = 0;
+    std::vector<void*> allocs;
+    int device = 0;
+    // host-buffer pipeline (created on first cfft_execute_host)
+    std::mutex host_mu;
+    bool host_ready = false;
+    int64_t host_chunk = 0;
+    void* host_buf[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t host_st[3] = {nullptr, nullptr, nullptr};   // in, compute, out
+    cudaEvent_t ev_in[3], ev_comp[3], ev_out[3];
+};
+
+static size_t elem_bytes(int dtype) { return dtype == CFFT_C128 ? 16 : 8; }
+static const size_t kSmemMax = 220 * 1024;
+static const size_t kSmemTwoPerSM = 110 * 1024;
+
+static std::string join(const std::vector<int>& v) {
+    std::string s;
+    for (size_t i = 0; i < v.size(); i++) s += (i ? "," : "") + std::to_string(v[i]);
+    return s;
+}
+
+// ------------------------------------------------------------ shape choice
+static bool rows_shape(int64_t M, int64_t nx, int conv, int dtype, int64_t batch, Shape& sh) {
+    if (M > 4096) return false;
+    auto rc = radix_split(M);
+    if (M > 1 && rc.empty()) return false;
+    if (wave_G(rc, M, CFFT_THREADS) < 1) return false;
+    size_t e = elem_bytes(dtype);
+    int64_t PC = M + ((M % 2 == 0) ? 1 : 0);
+    int64_t XP = (conv == CONV_RADER) ? nx : 0;
+    size_t per_row = (size_t)(PC + XP) * e;
+    // rows per CTA: ~48 KB of smem, but keep >= ~2 CTAs per SM busy
+    int64_t V = std::max<int64_t>(1, (int64_t)(48 * 1024) / (int64_t)per_row);
+    int64_t need = (batch + 295) / 296;
+    V = std::max<int64_t>(1, std::min<int64_t>(V, need));
+    sh.mode = MODE_ROWS;
+    sh.M = M;
+    sh.V = (int)V;
+    sh.rc = rc;
+    sh.smem = (size_t)V * per_row + 64 * sizeof(double2) + 16;
+    return sh.smem <= kSmemMax;
+}
+
+static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vector<Shape>& out) {
+    size_t e = elem_bytes(dtype);
+    for (int64_t N1 = 2; N1 <= 4096; N1++) {
+        if (M % N1) continue;
+        int64_t N2 = M / N1;
+        if (N2 < 2 || N2 > 4096) continue;
+        auto ra = radix_split(N1), rc = radix_split(N2);
+        if (ra.empty() || rc.empty()) continue;
+        if (wave_G(ra, N1, CFFT_THREADS) < 1 || wave_G(rc, N2, CFFT_THREADS) < 1) continue;
+        for (int C = 1; C <= 16; C++) {
+            if (N1 % C || N2 % C) continue;
+            int64_t W = N2 / C, R1 = N1 / C;
+            int64_t PA, PC;
+            if (C == 1) {
+                PA = PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
+            } else {
+                if (M / C > (int64_t)CFFT_THREADS * CFFT_EMAX) continue;
+                if (W < 2 || R1 < 2) continue;
+                PA = W;
+                PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
+            }
+            int64_t XP = (conv == CONV_RADER) ? (nx + C - 1) / C : 0;
+            int64_t bufsz = std::max(N1 * PA, R1 * PC);
+            size_t smem = (size_t)(bufsz + XP) * e + (32 + 16) * sizeof(double2) + 16;
+            if (smem > kSmemMax) continue;
+            Shape sh;
+            sh.mode = MODE_FOUR;
+            sh.conv = conv;
+            sh.M = M;
+            sh.N1 = (int)N1;
+            sh.N2 = (int)N2;
+            sh.C = C;
+            sh.ra = ra;
+            sh.rc = rc;
+            sh.smem = smem;
+            double bal = std::fabs(std::log2((double)N1 / (double)N2));
+            sh.score = (smem > kSmemTwoPerSM ? 8.0 : 0.0) + (C > 8 ? 3.0 : 0.0) + 0.6 * C +
+                       0.5 * bal + 0.1 * (ra.size() + rc.size());
+            out.push_back(sh);
+        }
+    }
+    std::sort(out.begin(), out.end(), [](const Shape& a, const Shape& b) { return a.score < b.score; });
+}
+
+static bool global_shape(int64_t M, int dtype, Shape& sh) {
+    size_t e = elem_bytes(dtype);
+    int64_t best = -1;
+    double bestb = 1e9;
+    for (int64_t N1 = 2; N1 <= 4096; N1++) {
+        if (M % N1) continue;
+        int64_t N2 = M / N1;
+        if (N2 < 2 || N2 > 4096) continue;
+        auto ra = radix_split(N1), rc = radix_split(N2);
+        if (ra.empty() || rc.empty()) continue;
+        if (wave_G(ra, N1, CFFT_THREADS) < 1 || wave_G(rc, N2, CFFT_THREADS) < 1) continue;
+        double b = std::fabs(std::log2((double)N1 / (double)N2));
+        if (b < bestb) { bestb = b; best = N1; }
+    }
+    if (best < 0) return false;
+    sh.mode = MODE_COLPASS;
+    sh.M = M;
+    sh.N1 = (int)best;
+    sh.N2 = (int)(M / best);
+    sh.ra = radix_split(sh.N1);
+    sh.rc = radix_split(sh.N2);
+    (void)e;
+    return true;
+}
+
+// conv length for a non-smooth n
+static void conv_kind(int64_t n, int& conv, int64_t& M) {
+    if (is_smooth7(n)) { conv = CONV_NONE; M = n; return; }
+    if (is_prime64(n)) { conv = CONV_RADER; M = smooth_ceil(2 * n - 3); return; }
+    conv = CONV_BLUE;
+    M = smooth_ceil(2 * n - 1);
+}
+
+static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) {
+    std::vector<Shape> v;
+    int conv;
+    int64_t M;
+    conv_kind(n, conv, M);
+    Shape sh;
+    if (rows_shape(M, n, conv, dtype, batch, sh)) {
+        sh.conv = conv;
+        v.push_back(sh);
+    }
+    if (M > 64) four_candidates(M, n, conv, dtype, v);
+    if (v.empty()) {
+        // beyond a cluster: two HBM passes; Rader here becomes Bluestein
+        int c2 = conv;
+        int64_t M2 = M;
+        if (conv == CONV_RADER) { c2 = CONV_BLUE; M2 = smooth_ceil(2 * n - 1); }
+        Shape g;
+        if (global_shape(M2, dtype, g)) {
+            g.conv = c2;
+            v.push_back(g);
+        }
+    }
+    return v;
+}
+
+static std::string shape_desc(const Shape& s, int64_t n) {
+    std::string c = s.conv == CONV_RADER ? "rader" : s.conv == CONV_BLUE ? "bluestein" : "";
+    std::string pre = c.empty() ? "" : c + "(n=" + std::to_string(n) + ",M=" + std::to_string(s.M) + ")+";
+    if (s.mode == MODE_ROWS)
+        return pre + "rows(V=" + std::to_string(s.V) + ")[" + join(s.rc) + "]";
+    if (s.mode == MODE_FOUR)
+        return pre + "four(C=" + std::to_string(s.C) + ",N1=" + std::to_string(s.N1) +
+               ",N2=" + std::to_string(s.N2) + ")[" + join(s.ra) + "|" + join(s.rc) + "]";
+    return pre + "twopass(N1=" + std::to_string(s.N1) + ",N2=" + std::to_string(s.N2) + ")[" +
+           join(s.ra) + "|" + join(s.rc) + "]";
+}
+
+// ---------------------------------------------------------- device tables
+static int dev_upload(cfft_plan_s* P, const void* h, size_t bytes, void** d) {
+    CUDA_TRY(cudaMalloc(d, bytes));
+    P->allocs.push_back(*d);
+    CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
+    return CFFT_OK;
+}
+static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, SubPlan& sp) {
+    memset(&sp, 0, sizeof sp);
+    sp.L = (int)L;
+    sp.np = (int)rad.size();
+    if (sp.np > CFFT_MAXP) return fail(CFFT_ERR_UNSUPPORTED, "too many radix passes");
+    for (int i = 0; i < sp.np; i++) sp.radix[i] = (unsigned char)rad[i];
+    sp.G = std::max(1, wave_G(rad, L, CFFT_THREADS));
+    if (L <= 1) { sp.tw = nullptr; return CFFT_OK; }
+    void* d = nullptr;
+    int rc;
+    if (P->dtype == CFFT_C128) {
+        std::vector<double2> t(L);
+        for (int64_t m = 0; m < L; m++) t[m] = omega(m, L, -1);
+        rc = dev_upload(P, t.data(), t.size() * sizeof(double2), &d);
+    } else {
+        std::vector<float2> t(L);
+        for (int64_t m = 0; m < L; m++) {
+            double2 w = omega(m, L, -1);
+            t[m] = make_float2((float)w.x, (float)w.y);
+        }
+        rc = dev_upload(P, t.data(), t.size() * sizeof(float2), &d);
+    }
+    sp.tw = d;
+    return rc;
+}
+static int make_twolevel(cfft_plan_s* P, int64_t N, TwoLevel& t) {
+    int bits = 0;
+    while ((1LL << (2 * bits)) < N) bits++;
+    int64_t lo_n = 1LL << bits, hi_n = (N + lo_n - 1) / lo_n + 1;
+    std::vector<double2> lo(lo_n), hi(hi_n);
+    for (int64_t a = 0; a < lo_n; a++) lo[a] = omega(a, N, -1);
+    for (int64_t b = 0; b < hi_n; b++) hi[b] = omega(b * lo_n, N, -1);
+    void *dl, *dh;
+    int rc = dev_upload(P, lo.data(), lo.size() * sizeof(double2), &dl);
+    if (rc) return rc;
+    rc = dev_upload(P, hi.data(), hi.size() * sizeof(double2), &dh);
+    if (rc) return rc;
+    t.lo = (const double2*)dl;
+    t.hi = (const double2*)dh;
+    t.bits = bits;
+    t.N = (int)N;
+    return CFFT_OK;
+}
+
+static int plan_build(cfft_plan_s* P, const Shape& sh);
+static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cudaStream_t st,
+                        int64_t nbatch = -1);
+static void plan_free(cfft_plan_s* P);
+
+// spectrum = FFT_M(b) / M in FP64 using this library's own C128 path
+static int conv_spectrum(cfft_plan_s* P, int64_t M, const std::vector<double2>& b, const double2** out) {
+    cfft_plan_s sub;
+    sub.n = M;
+    sub.batch = 1;
+    sub.dtype = CFFT_C128;
+    sub.flags = 0;
+    auto cands = candidate_shapes(M, CFFT_C128, 1);
+    if (cands.empty()) return fail(CFFT_ERR_UNSUPPORTED, "no shape for convolution length");
+    int rc = CFFT_ERR_UNSUPPORTED;
+    for (auto& c : cands) {
+        rc = plan_build(&sub, c);
+        if (rc == CFFT_OK) break;
+        plan_free(&sub);
+    }
+    if (rc) return rc;
+    void *din = nullptr, *dout = nullptr;
+    rc = dev_upload(P, b.data(), M * sizeof(double2), &din);
+    if (rc) { plan_free(&sub); return rc; }
+    CUDA_TRY(cudaMalloc(&dout, M * sizeof(double2)));
+    P->allocs.push_back(dout);
+    rc = plan_execute(&sub, din, dout, CFFT_FORWARD, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    plan_free(&sub);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(CFFT_ERR_CUDA, std::string("spectrum: ") + cudaGetErrorString(e));
+    std::vector<double2> h(M);
+    CUDA_TRY(cudaMemcpy(h.data(), dout, M * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (auto& v : h) { v.x /= (double)M; v.y /= (double)M; }
+    CUDA_TRY(cudaMemcpy(dout, h.data(), M * sizeof(double2), cudaMemcpyHostToDevice));
+    *out = (const double2*)dout;
+    return CFFT_OK;
+}
+
+static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp) {
+    const int64_t n = P->n, M = sh.M;
+    std::vector<double2> b(M, make_double2(0, 0));
+    if (sh.conv == CONV_RADER) {
+        const int64_t L = n - 1, g = primitive_root(n), ginv = powmod(g, n - 2, n);
+        std::vector<int> perm(L), iperm(L);
+        int64_t a = 1, c = 1;
+        for (int64_t i = 0; i < L; i++) {
+            perm[i] = (int)a;
+            iperm[i] = (int)c;
+            a = (int64_t)(((__int128)a * g) % n);
+            c = (int64_t)(((__int128)c * ginv) % n);
+        }
+        // W[m] = w^(-g^-m): the reference's twiddles (prime.jl:36-37) or exact
+        std::vector<double2> W(L);
+        if (P->flags & CFFT_EXACT_TWIDDLES) {
+            for (int64_t m = 0; m < L; m++) W[m] = omega(iperm[m], n, -1);
+        } else {
+            double2 w = omega(1, n, +1);                 // cispi(2/n)
+            {
+                // cispi(T(2/n)) evaluates at the rounded argument 2/n
+                double arg = 2.0 / (double)n;            // in units of pi
+                long double x = 3.141592653589793238462643383279502884L * (long double)arg;
+                w = make_double2((double)cosl(x), (double)sinl(x));
+            }
+            double2 winv = julia_inv(w);
+            for (int64_t m = 0; m < L; m++) W[m] = pow_by_squaring(winv, iperm[m]);
+        }
+        for (int64_t m = 0; m < L; m++) b[m] = W[m];
+        for (int64_t m = 1; m < L; m++) b[M - L + m] = W[m];
+        void *dp, *di;
+        int rc = dev_upload(P, perm.data(), L * sizeof(int), &dp);
+        if (rc) return rc;
+        rc = dev_upload(P, iperm.data(), L * sizeof(int), &di);
+        if (rc) return rc;
+        kp.perm = (const int*)dp;
+        kp.iperm = (const int*)di;
+    } else {
+        // chirp[j] = exp(-i pi j^2 / n); b[m] = conj(chirp[|m|])
+        std::vector<double2> ch(n);
+        for (int64_t j = 0; j < n; j++) {
+            int64_t e = (int64_t)(((__int128)j * j) % (2 * n));
+            ch[j] = omega(e, 2 * n, -1);
+        }
+        for (int64_t m = 0; m < n; m++) b[m] = make_double2(ch[m].x, -ch[m].y);
+        for (int64_t m = 1; m < n; m++) b[M - m] = make_double2(ch[m].x, -ch[m].y);
+        void* dc;
+        int rc = dev_upload(P, ch.data(), n * sizeof(double2), &dc);
+        if (rc) return rc;
+        kp.chirp = (const double2*)dc;
+    }
+    return conv_spectrum(P, M, b, &kp.spec);
+}
+
+static int plan_build(cfft_plan_s* P, const Shape& sh) {
+    P->shape = sh;
+    P->stages.clear();
+    P->desc = shape_desc(sh, P->n);
+    const size_t e = elem_bytes(P->dtype);
+    KParams kp;
+    memset(&kp, 0, sizeof kp);
+    kp.conv = sh.conv;
+    kp.nx = (int)P->n;
+    kp.M = (int)sh.M;
+    int rc;
+    if (sh.conv != CONV_NONE) {
+        rc = make_conv_tables(P, sh, kp);
+        if (rc) return rc;
+    }
+    if (sh.mode == MODE_ROWS) {
+        kp.mode = MODE_ROWS;
+        kp.V = sh.V;
+        kp.PC = (int)(sh.M + ((sh.M % 2 == 0) ? 1 : 0));
+        kp.XP = (sh.conv == CONV_RADER) ? (int)P->n : 0;
+        rc = make_subplan(P, sh.M, sh.rc, kp.pc);
+        if (rc) return rc;
+        Stage s;
+        s.kp = kp;
+        s.threads = CFFT_THREADS;
+        s.smem = sh.smem;
+        s.cluster = 1;
+        s.grid = 0;  // set per execution from batch
+        s.in_sel = 0;
+        s.out_sel = 1;
+        CUDA_TRY(cfft_prepare_kernel(MODE_ROWS, P->dtype, s.smem, 1));
+        P->stages.push_back(s);
+        P->chunk = P->batch;
+        return CFFT_OK;
+    }
+    if (sh.mode == MODE_FOUR) {
+        kp.mode = MODE_FOUR;
+        kp.N1 = sh.N1;
+        kp.N2 = sh.N2;
+        kp.C = sh.C;
+        if (sh.C == 1) {
+            kp.PA = kp.PC = sh.N2 + ((sh.N2 % 2 == 0) ? 1 : 0);
+        } else {
+            kp.PA = sh.N2 / sh.C;
+            kp.PC = sh.N2 + ((sh.N2 % 2 == 0) ? 1 : 0);
+        }
+        kp.XP = (sh.conv == CONV_RADER) ? (int)((P->n + sh.C - 1) / sh.C) : 0;
+        rc = make_subplan(P, sh.N1, sh.ra, kp.pa);
+        if (rc) return rc;
+        rc = make_subplan(P, sh.N2, sh.rc, kp.pc);
+        if (rc) return rc;
+        rc = make_twolevel(P, sh.M, kp.t4);
+        if (rc) return rc;
+        Stage s;
+        s.kp = kp;
+        s.threads = CFFT_THREADS;
+        s.smem = sh.smem;
+        s.cluster = sh.C;
+        s.grid = 0;
+        s.in_sel = 0;
+        s.out_sel = 1;
+        CUDA_TRY(cfft_prepare_kernel(MODE_FOUR, P->dtype, s.smem, sh.C));
+        if (sh.C > 1) {
+            int nclusters = 0;
+            cudaError_t ce = cfft_max_active_clusters(MODE_FOUR, P->dtype, CFFT_THREADS, s.smem, sh.C,
+                                                      &nclusters);
+            if (ce != cudaSuccess || nclusters < 1) {
+                cudaGetLastError();
+                return fail(CFFT_ERR_UNSUPPORTED, "cluster configuration not schedulable: C=" +
+                                                      std::to_string(sh.C));
+            }
+        }
+        P->stages.push_back(s);
+        P->chunk = P->batch;
+        return CFFT_OK;
+    }
+    // two HBM passes per FFT_M (and two FFT_M for a convolution)
+    const int64_t N1 = sh.N1, N2 = sh.N2, M = sh.M;
+    SubPlan pa, pc;
+    rc = make_subplan(P, N1, sh.ra, pa);
+    if (rc) return rc;
+    rc = make_subplan(P, N2, sh.rc, pc);
+    if (rc) return rc;
+    TwoLevel t4;
+    rc = make_twolevel(P, M, t4);
+    if (rc) return rc;
+    // tile widths: largest divisor with <= 96 KB of smem
+    auto pick_tile = [&](int64_t count, int64_t per) {
+        int64_t best = 1;
+        for (int64_t v = 1; v <= count; v++)
+            if (count % v == 0 && (size_t)(v * per) * e <= 96 * 1024 && v <= 64) best = v;
+        return best;
+    };
+    const int64_t PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
+    const int64_t Vc = pick_tile(N2, N1), Vr = pick_tile(N1, PC);
+    // chunk the batch so the scratch of one chunk stays within ~64 MB (L2 sized)
+    const int nscr = (sh.conv == CONV_NONE) ? 1 : 2;
+    int64_t chunk = std::max<int64_t>(1, (int64_t)(64LL << 20) / (int64_t)(M * e * nscr));
+    chunk = std::min<int64_t>(chunk, P->batch);
+    P->chunk = chunk;
+    P->scratch_bytes = (size_t)chunk * M * e;
+    for (int i = 0; i < nscr; i++) {
+        CUDA_TRY(cudaMalloc(&P->scratch[i], P->scratch_bytes));
+        P->allocs.push_back(P->scratch[i]);
+    }
+    auto col = [&](int pre, int in_sel, int out_sel) {
+        Stage s;
+        s.kp = kp;
+        s.kp.mode = MODE_COLPASS;
+        s.kp.N1 = (int)N1;
+        s.kp.N2 = (int)N2;
+        s.kp.V = (int)Vc;
+        s.kp.PA = (int)Vc;
+        s.kp.pa = pa;
+        s.kp.t4 = t4;
+        s.kp.pre = pre;
+        s.threads = CFFT_THREADS;
+        s.smem = (size_t)(N1 * Vc) * e + 16;
+        s.cluster = 1;
+        s.in_sel = in_sel;
+        s.out_sel = out_sel;
+        return s;
+    };
+    auto row = [&](int post, int in_sel, int out_sel) {
+        Stage s;
+        s.kp = kp;
+        s.kp.mode = MODE_ROWPASS;
+        s.kp.N1 = (int)N1;
+        s.kp.N2 = (int)N2;
+        s.kp.V = (int)Vr;
+        s.kp.PC = (int)PC;
+        s.kp.pc = pc;
+        s.kp.post = post;
+        s.threads = CFFT_THREADS;
+        s.smem = (size_t)(Vr * PC) * e + 16;
+        s.cluster = 1;
+        s.in_sel = in_sel;
+        s.out_sel = out_sel;
+        return s;
+    };
+    if (sh.conv == CONV_NONE) {
+        P->stages.push_back(col(PRE_NONE, 0, 2));
+        P->stages.push_back(row(POST_OUT, 2, 1));
+    } else {
+        P->stages.push_back(col(PRE_CHIRP, 0, 2));
+        P->stages.push_back(row(POST_RAW, 2, 3));
+        P->stages.push_back(col(PRE_SPEC, 3, 2));
+        P->stages.push_back(row(POST_CHIRP, 2, 1));
+    }
+    for (auto& s : P->stages) CUDA_TRY(cfft_prepare_kernel(s.kp.mode, P->dtype, s.smem, 1));
+    return CFFT_OK;
+}
+
+static void plan_free(cfft_plan_s* P) {
+    if (P->host_ready) {
+        for (int i = 0; i < 3; i++) {
+            cudaFree(P->host_buf[i]);
+            cudaStreamDestroy(P->host_st[i]);
+            cudaEventDestroy(P->ev_in[i]);
+            cudaEventDestroy(P->ev_comp[i]);
+            cudaEventDestroy(P->ev_out[i]);
+            P->host_buf[i] = nullptr;
+        }
+        P->host_ready = false;
+    }
+    for (void* p : P->allocs) cudaFree(p);
+    P->allocs.clear();
+    P->stages.clear();
+    P->scratch[0] = P->scratch[1] = nullptr;
+}
+
+static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cudaStream_t st,
+                        int64_t nbatch) {
+    if (dir < 0 || dir > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    const size_t e = elem_bytes(P->dtype);
+    const int64_t n = P->n;
+    const int64_t total = (nbatch < 0) ? P->batch : std::min(nbatch, P->batch);
+    for (int64_t b0 = 0; b0 < total; b0 += P->chunk) {
+        const int64_t nb = std::min(P->chunk, total - b0);
+        for (auto& s : P->stages) {
+            KParams kp = s.kp;
+            kp.dir = dir;
+            kp.scale = (dir == CFFT_INVERSE) ? 1.0 / (double)n : 1.0;
+            kp.batch = (int)nb;
+            const char* user_in = (const char*)in + (size_t)b0 * n * e;
+            char* user_out = (char*)out + (size_t)b0 * n * e;
+            auto sel = [&](int w) -> void* {
+                return w == 0 ? (void*)user_in : w == 1 ? (void*)user_out : P->scratch[w - 2];
+            };
+            kp.in = sel(s.in_sel);
+            kp.out = sel(s.out_sel);
+            kp.in_dist = (s.in_sel >= 2) ? P->shape.M : n;
+            kp.out_dist = (s.out_sel >= 2) ? P->shape.M : n;
+            unsigned grid;
+            if (kp.mode == MODE_ROWS) grid = (unsigned)((nb + kp.V - 1) / kp.V);
+            else if (kp.mode == MODE_FOUR) grid = (unsigned)(nb * kp.C);
+            else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
+            else grid = (unsigned)(nb * (kp.N1 / kp.V));
+            cudaError_t ce = cfft_launch(kp, P->dtype, grid, s.threads, s.smem, s.cluster, st);
+            if (ce != cudaSuccess)
+                return fail(CFFT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
+        }
+    }
+    return CFFT_OK;
+}
+
+// ------------------------------------------------------- autotune (MEASURE)
+static float time_plan(cfft_plan_s* P, void* buf) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    plan_execute(P, buf, buf, 0, 0);
+    cudaEventRecord(a, 0);
+    const int reps = 3;
+    for (int i = 0; i < reps; i++) plan_execute(P, buf, buf, 0, 0);
+    cudaEventRecord(b, 0);
+    cudaError_t ce = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ce != cudaSuccess) { cudaGetLastError(); return 1e30f; }
+    return ms / reps;
+}
+
+static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dtype, int flags) {
+    if (!out) return fail(CFFT_ERR_INVALID, "plan pointer is null");
+    if (n < 1 || batch < 1) return fail(CFFT_ERR_INVALID, "n and batch must be >= 1");
+    if (dtype != CFFT_C128 && dtype != CFFT_C64) return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128 or CFFT_C64");
+    if (n > (1LL << 26)) return fail(CFFT_ERR_UNSUPPORTED, "n above 2^26 is not supported");
+    int level = flags & 3;
+    if (level > 2) return fail(CFFT_ERR_INVALID, "flag must be NO_FLAG, MEASURE or ENCHANT");
+    auto cands = candidate_shapes(n, dtype, batch);
+    if (cands.empty()) return fail(CFFT_ERR_UNSUPPORTED, "no execution shape for n=" + std::to_string(n));
+    cfft_plan_s* P = new cfft_plan_s();
+    P->n = n;
+    P->batch = batch;
+    P->dtype = dtype;
+    P->flags = flags;
+    cudaGetDevice(&P->device);
+    int rc = CFFT_ERR_UNSUPPORTED;
+    if (level == CFFT_NO_FLAG) {
+        for (auto& c : cands) {
+            rc = plan_build(P, c);
+            if (rc == CFFT_OK) break;
+            plan_free(P);
+        }
+    } else {
+        // MEASURE: the best few heuristic candidates; ENCHANT: all of them
+        size_t limit = (level == CFFT_MEASURE) ? std::min<size_t>(cands.size(), 4) : cands.size();
+        limit = std::min<size_t>(limit, 24);
+        const size_t e = elem_bytes(dtype);
+        void* buf = nullptr;
+        if (cudaMalloc(&buf, (size_t)n * batch * e) != cudaSuccess) {
+            delete P;
+            return fail(CFFT_ERR_NOMEM, "autotune buffer allocation failed");
+        }
+        cudaMemset(buf, 0, (size_t)n * batch * e);
+        float best = 1e30f;
+        int best_i = -1;
+        for (size_t i = 0; i < limit; i++) {
+            if (plan_build(P, cands[i]) == CFFT_OK) {
+                float t = time_plan(P, buf);
+                if (t < best) { best = t; best_i = (int)i; }
+            }
+            plan_free(P);
+        }
+        cudaFree(buf);
+        if (best_i < 0) { delete P; return fail(CFFT_ERR_UNSUPPORTED, "no candidate plan ran"); }
+        rc = plan_build(P, cands[best_i]);
+    }
+    if (rc != CFFT_OK) {
+        std::string keep = g_err;
+        plan_free(P);
+        delete P;
+        g_err = keep;
+        return rc;
+    }
+    *out = P;
+    return CFFT_OK;
+}
+
+// ------------------------------------------------------------------- C ABI
+static std::mutex g_cache_mu;
+static std::map<std::tuple<int, int64_t, int64_t, int, int>, cfft_plan_s*> g_cache;
+
+extern "C" {
+
+int cfft_version(void) { return 100; }
+
+const char* cfft_last_error(void) { return g_err.c_str(); }
+
+int cfft_plan_create(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags) {
+    g_err.clear();
+    return plan_create_impl(plan, n, batch, dtype, flags);
+}
+
+int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, void* stream) {
+    if (!plan || !d_in || !d_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
+    return plan_execute(plan, d_in, d_out, direction, (cudaStream_t)stream);
+}
+
+int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int direction) {
+    if (!plan || !h_in || !h_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
+    if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    cfft_plan_s* P = plan;
+    std::lock_guard<std::mutex> lk(P->host_mu);
+    const size_t e = elem_bytes(P->dtype);
+    const size_t tbytes = (size_t)P->n * e;
+    if (!P->host_ready) {
+        // ~32 MB chunks, a multiple of the plan's own chunk when it has scratch
+        int64_t c = std::max<int64_t>(1, (int64_t)(32LL << 20) / (int64_t)tbytes);
+        c = std::min<int64_t>(c, P->batch);
+        if (P->chunk > 0 && P->chunk < P->batch) c = std::max<int64_t>(P->chunk, (c / P->chunk) * P->chunk);
+        P->host_chunk = std::min<int64_t>(c, P->batch);
+        for (int i = 0; i < 3; i++) {
+            CUDA_TRY(cudaMalloc(&P->host_buf[i], (size_t)P->host_chunk * tbytes));
+            CUDA_TRY(cudaStreamCreateWithFlags(&P->host_st[i], cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&P->ev_in[i], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&P->ev_comp[i], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&P->ev_out[i], cudaEventDisableTiming));
+        }
+        P->host_ready = true;
+    }
+    // three-stage pipeline: H2D (stream 0) -> transform (stream 1) -> D2H
+    // (stream 2) over a ring of three device chunk buffers
+    cudaStream_t sin = P->host_st[0], scomp = P->host_st[1], sout = P->host_st[2];
+    int64_t i = 0;
+    for (int64_t b0 = 0; b0 < P->batch; b0 += P->host_chunk, i++) {
+        const int64_t nb = std::min(P->host_chunk, P->batch - b0);
+        const int k = (int)(i % 3);
+        const size_t off = (size_t)b0 * tbytes, bytes = (size_t)nb * tbytes;
+        if (i >= 3) CUDA_TRY(cudaStreamWaitEvent(sin, P->ev_out[k], 0));
+        CUDA_TRY(cudaMemcpyAsync(P->host_buf[k], (const char*)h_in + off, bytes, cudaMemcpyHostToDevice, sin));
+        CUDA_TRY(cudaEventRecord(P->ev_in[k], sin));
+        CUDA_TRY(cudaStreamWaitEvent(scomp, P->ev_in[k], 0));
+        int rc = plan_execute(P, P->host_buf[k], P->host_buf[k], direction, scomp, nb);
+        if (rc) { cudaStreamSynchronize(scomp); return rc; }
+        CUDA_TRY(cudaEventRecord(P->ev_comp[k], scomp));
+        CUDA_TRY(cudaStreamWaitEvent(sout, P->ev_comp[k], 0));
+        CUDA_TRY(cudaMemcpyAsync((char*)h_out + off, P->host_buf[k], bytes, cudaMemcpyDeviceToHost, sout));
+        CUDA_TRY(cudaEventRecord(P->ev_out[k], sout));
+    }
+    CUDA_TRY(cudaStreamSynchronize(sout));
+    CUDA_TRY(cudaStreamSynchronize(scomp));
+    return CFFT_OK;
+}
+
+int cfft_plan_destroy(cfft_plan plan) {
+    if (!plan) return fail(CFFT_ERR_INVALID, "null plan");
+    plan_free(plan);
+    delete plan;
+    return CFFT_OK;
+}
+
+int cfft_fft(int64_t n, int64_t batch, int dtype, int flags, const void* d_in, void* d_out,
+             int direction, void* stream) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cfft_plan_s* P = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        auto key = std::make_tuple(dev, n, batch, dtype, flags);
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) {
+            P = it->second;
+        } else {
+            int rc = plan_create_impl(&P, n, batch, dtype, flags);
+            if (rc) return rc;
+            g_cache[key] = P;
+        }
+    }
+    return cfft_execute(P, d_in, d_out, direction, stream);
+}
+
+int cfft_empty_cache(void) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto& kv : g_cache) {
+        plan_free(kv.second);
+        delete kv.second;
+    }
+    g_cache.clear();
+    return CFFT_OK;
+}
+
+int cfft_plan_describe(cfft_plan plan, char* buf, int len) {
+    if (!plan || !buf || len < 1) return fail(CFFT_ERR_INVALID, "bad describe arguments");
+    snprintf(buf, (size_t)len, "%s", plan->desc.c_str());
+    return CFFT_OK;
+}
+
+int cfft_describe_strategy(int64_t n, int dtype, char* buf, int len) {
+    if (n < 1 || !buf || len < 1) return fail(CFFT_ERR_INVALID, "bad describe arguments");
+    auto c = candidate_shapes(n, dtype, 1);
+    if (c.empty()) return fail(CFFT_ERR_UNSUPPORTED, "no shape");
+    snprintf(buf, (size_t)len, "%s", shape_desc(c[0], n).c_str());
+    return CFFT_OK;
+}
+
+int64_t cfft_plan_workspace_bytes(cfft_plan plan) {
+    if (!plan) return -1;
+    return (int64_t)plan->scratch_bytes * ((plan->scratch[1] != nullptr) ? 2 : (plan->scratch[0] ? 1 : 0));
+}
+
+int cfft_plan_launches(cfft_plan plan) {
+    if (!plan) return -1;
+    int64_t chunks = (plan->batch + plan->chunk - 1) / plan->chunk;
+    return (int)(chunks * (int64_t)plan->stages.size());
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+/*
+ * catabra_b200.h -- C ABI of the B200-native 1D complex FFT.
+ *
+ * Drop-in boundary for CatabraFFT.jl's public FFT path.  Every entry point is
+ * plain C (pointers, sizes, status codes); no exception or abort crosses it.
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the CatabraFFT.jl project).
+ *
+ * Data layout: interleaved complex, contiguous, `batch` transforms of length
+ * n back to back ([batch][n]); CFFT_C128 = ComplexF64 (16 B per element),
+ * CFFT_C64 = ComplexF32 (8 B per element).
+ *
+ * Threading: plans are immutable after creation; one plan may be executed
+ * concurrently on different streams as long as each concurrent call uses
+ * its own output buffer (plans whose strategy needs device scratch -- see
+ * cfft_plan_workspace_bytes -- serialise on that scratch: give each stream
+ * its own plan).  Inputs are never modified (the reference's p * x can
+ * overwrite x, src/CatabraFFT.jl:186-196).
+ */
+#ifndef CATABRA_B200_H
+#define CATABRA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* element types: the reference's Complex{T}, T in {Float64, Float32} */
+enum { CFFT_C128 = 0, CFFT_C64 = 1 };
+
+/* directions: fft (CatabraFFT.jl:65-72), ifft with 1/n (:88-101),
+ * bfft without scaling (:103-115) */
+enum { CFFT_FORWARD = 0, CFFT_INVERSE = 1, CFFT_BACKWARD = 2 };
+
+/* planner flags, same values as the reference's FLAG (src/spells.jl:4-8):
+ * NO_FLAG = heuristic plan, MEASURE = time candidate plans on the device,
+ * ENCHANT = wider timed search (factorisations x cluster sizes x radix
+ * orders).  Bit 4 (CFFT_EXACT_TWIDDLES) replaces the reference's Rader
+ * twiddle recurrence (src/prime.jl:36-37) by exactly rounded twiddles. */
+enum { CFFT_NO_FLAG = 0, CFFT_MEASURE = 1, CFFT_ENCHANT = 2, CFFT_EXACT_TWIDDLES = 16 };
+
+/* status codes */
+enum {
+    CFFT_OK = 0,
+    CFFT_ERR_INVALID = 1,     /* bad argument (n < 1, batch < 1, null pointer, ...) */
+    CFFT_ERR_CUDA = 2,        /* a CUDA call failed; cfft_last_error() has the text  */
+    CFFT_ERR_NOMEM = 3,       /* device or host allocation failed                    */
+    CFFT_ERR_UNSUPPORTED = 4  /* size or configuration outside what the build covers */
+};
+
+typedef struct cfft_plan_s* cfft_plan;
+
+/* Replaces plan_fft(x, flag) -> Spell (src/CatabraFFT.jl:149-167) and the
+ * strategy choice of generate_and_cache_fft! (src/kernel.jl:72-92).
+ * Builds twiddle tables, Rader/Bluestein spectra and scratch on the current
+ * device.  batch >= 1 transforms of length n per execution. */
+int cfft_plan_create(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags);
+
+/* Replaces mul!(y, p, x) / p * x (src/CatabraFFT.jl:186-196) and
+ * fft_kernel! (src/kernel.jl:95-100): device pointers, enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  in == out is allowed. */
+int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, void* stream);
+
+/* Replaces fft(x) / ifft(x) / bfft(x) (src/CatabraFFT.jl:65-115) for callers
+ * holding host memory (the Julia ccall path): copies in, transforms, copies
+ * out and synchronises.  Host buffers may be pageable or pinned. */
+int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int direction);
+
+/* Releases a plan and its device tables. */
+int cfft_plan_destroy(cfft_plan plan);
+
+/* One-call form with an internal plan cache keyed by (n, batch, dtype,
+ * flags), mirroring fft_kernel!'s cached lookup (src/kernel.jl:72-100). */
+int cfft_fft(int64_t n, int64_t batch, int dtype, int flags, const void* d_in, void* d_out,
+             int direction, void* stream);
+
+/* Replaces empty_cache() (src/CatabraFFT.jl:39-43): frees cached plans. */
+int cfft_empty_cache(void);
+
+/* Thread-local text of the last error on this thread ("" if none). */
+const char* cfft_last_error(void);
+
+/* Plan introspection: strategy string, e.g.
+ * "four(C=12,N1=180,N2=168)[8,9,5,4|8,7,3]"; no device work. */
+int cfft_plan_describe(cfft_plan plan, char* buf, int len);
+
+/* Planner decision for (n, dtype) without touching the GPU (host logic only,
+ * usable on machines without a device). */
+int cfft_describe_strategy(int64_t n, int dtype, char* buf, int len);
+
+/* Bytes of device scratch a plan holds beyond its tables (0 for the
+ * one-HBM-round-trip strategies). */
+int64_t cfft_plan_workspace_bytes(cfft_plan plan);
+
+/* Number of kernel launches one cfft_execute of this plan issues. */
+int cfft_plan_launches(cfft_plan plan);
+
+/* ABI version (major*100 + minor). */
+int cfft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CATABRA_B200_H */

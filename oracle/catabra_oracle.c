@@ -402,10 +402,20 @@ static cx power_by_squaring(cx x, int64_t p) {
     }
     return y;
 }
-/* inv(z) for |z| ~ 1 (Julia's robust complex inverse reduces to conj(z)/|z|^2) */
+/* inv(z): Julia Base's robust complex inverse (Smith's algorithm; the
+ * rescaling branches of Base.inv never trigger for |z| ~ 1). */
 static cx cinv(cx z) {
-    REAL d = z.re * z.re + z.im * z.im;
-    return C(z.re / d, -z.im / d);
+    REAL c = z.re, d = z.im;
+    if (fabs((double)c) >= fabs((double)d)) {
+        REAL r = d / c;
+        REAL t = (REAL)1 / (c + d * r);
+        return C(t, -r * t);
+    } else {
+        REAL cc = d, dd = c;
+        REAL r = dd / cc;
+        REAL t = (REAL)1 / (cc + dd * r);
+        return C(r * t, -t);
+    }
 }
 
 static node *build_plan(int64_t n) {
