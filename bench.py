@@ -184,14 +184,53 @@ def run_reference_arm(args):
     return 0
 
 
+def measure_e2e(torch, cb, lib, plans, bufs, args, world, dev):
+    """End to end through the C ABI host entry: pinned host buffers, the copies
+    inside the timed region, fwd + inv of both batches per step."""
+    host = []
+    for (x, _, _), (n, b) in zip(bufs, SIZES):
+        hin = torch.empty((b, n), dtype=torch.complex128, pin_memory=True)
+        hin.copy_(x.cpu())
+        host.append((hin, torch.empty_like(hin)))
+    torch.cuda.synchronize()
+    vp = ctypes.c_void_p
+    for h, (hin, hout) in zip(plans, host):          # warm the staging buffers
+        cb.check(lib.cfft_execute_host(h, vp(hin.data_ptr()), vp(hout.data_ptr()), 0))
+    steps = max(1, min(3, args.steps))
+    te = time.perf_counter()
+    for _ in range(steps):
+        for h, (hin, hout) in zip(plans, host):
+            cb.check(lib.cfft_execute_host(h, vp(hin.data_ptr()), vp(hout.data_ptr()), 0))
+            cb.check(lib.cfft_execute_host(h, vp(hout.data_ptr()), vp(hout.data_ptr()), 1))
+    e2e_s = (time.perf_counter() - te) / steps
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = tt.item()
+    # per step: 2 calls per batch, each copies the batch in and out
+    io_bytes = sum(2 * n * b * ELEM for n, b in SIZES)
+    return {"value": round(world * algorithmic_bytes_per_step() / e2e_s / 1e9, 4), "unit": "GB/s",
+            "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
+            "ms_per_step": round(e2e_s * 1e3, 3),
+            "path": "cfft_execute_host (C ABI), pinned host buffers, fwd+inv of each batch"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--only", type=int, default=0, help="restrict to one transform length")
+    ap.add_argument("--batch", type=int, default=0, help="override the batch (profiling cases)")
+    ap.add_argument("--quick", action="store_true", help="skip the e2e and CPU-baseline legs")
     args = ap.parse_args()
+    global SIZES
+    if args.only:
+        SIZES = [(n, b) for n, b in SIZES if n == args.only] or [(args.only, 1024)]
+    if args.batch:
+        SIZES = [(n, args.batch) for n, _ in SIZES]
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(3, args.warmup)
@@ -278,35 +317,10 @@ def main():
     peak, peak_kind = load_peaks()
     traffic = load_traffic().get(f"four_c128_n{n_dom}_b{b_dom}")
 
-    # end to end: through the C ABI host entry (pinned host buffers, copies
-    # inside the timed region, fwd + inv of both batches per step)
-    host = []
-    for (x, _, _), (n, b) in zip(bufs, SIZES):
-        hin = torch.empty((b, n), dtype=torch.complex128, pin_memory=True)
-        hin.copy_(x.cpu())
-        hout = torch.empty_like(hin)
-        host.append((hin, hout))
-    torch.cuda.synchronize()
-    e2e_steps = max(1, min(3, args.steps))
-    for h, (hin, hout) in zip(plans, host):
-        cb.check(lib.cfft_execute_host(h, ctypes.c_void_p(hin.data_ptr()), ctypes.c_void_p(hout.data_ptr()), 0))
-    te = time.perf_counter()
-    for _ in range(e2e_steps):
-        for h, (hin, hout) in zip(plans, host):
-            cb.check(lib.cfft_execute_host(h, ctypes.c_void_p(hin.data_ptr()), ctypes.c_void_p(hout.data_ptr()), 0))
-            cb.check(lib.cfft_execute_host(h, ctypes.c_void_p(hout.data_ptr()), ctypes.c_void_p(hout.data_ptr()), 1))
-    e2e_s = (time.perf_counter() - te) / e2e_steps
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = tt.item()
-    io_bytes = sum(2 * n * b * ELEM for n, b in SIZES)
-    e2e = {"value": round(world * algorithmic_bytes_per_step() / e2e_s / 1e9, 4), "unit": "GB/s",
-           "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
-           "path": "cfft_execute_host (C ABI), pinned host buffers, fwd+inv of both batches"}
+    e2e = None if args.quick else measure_e2e(torch, cb, lib, plans, bufs, args, world, dev)
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.quick:
         threads = os.cpu_count() or 1
         res = cpu_reference(threads, args.cpu_budget, steps=1)[0]
         cpu = {"value": round(res[0], 4), "unit": "GB/s", "cores": threads, "kind": "port",

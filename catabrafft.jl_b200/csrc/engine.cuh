@@ -36,6 +36,14 @@ namespace cg = cooperative_groups;
 #include "engine_types.h"
 
 // ------------------------------------------------------------------ helpers
+// Thread index read through volatile asm: index math derived from it cannot
+// be hoisted out of the persistent loops, where the hoisted values would stay
+// live across whole transforms and push the FP64 codelets into spills.
+__device__ __forceinline__ int opaque_tid() {
+    int v;
+    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(v));
+    return v;
+}
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -64,7 +72,8 @@ __device__ __forceinline__ void stg_stream(double2* p, double2 v) { __stcs(p, v)
 __device__ __forceinline__ void stg_stream(float2* p, float2 v) { __stcs(p, v); }
 
 __device__ __forceinline__ double2 tw_two(const TwoLevel& t, unsigned e) {
-    return cmul(__ldg(t.lo + (e & ((1u << t.bits) - 1))), __ldg(t.hi + (e >> t.bits)));
+    // plain loads: the tables may have been staged in shared memory
+    return cmul(t.lo[e & ((1u << t.bits) - 1)], t.hi[e >> t.bits]);
 }
 // multiply by the four-step twiddle, evaluated in FP64 and rounded once
 __device__ __forceinline__ double2 apply_tw(double2 v, const TwoLevel& t, unsigned e) {
@@ -88,75 +97,136 @@ template <> __device__ __forceinline__ float2 store_out<float2>(const KParams& p
     return make_float2(v.x * s, -v.y * s);
 }
 
+// ------------------------------------------------------- fast division
+// q = floor(n / d) as (n * m) >> 40 with m = ceil(2^40 / d): exact for
+// n < 2^24 and d <= 2^16 (the planner keeps every index and divisor there).
+__device__ __forceinline__ int fdiv(unsigned n, unsigned long long m) {
+    return (int)(((unsigned long long)n * m) >> 40);
+}
+__device__ __forceinline__ unsigned long long fdiv_magic(int d) {
+    return ((1ULL << 40) + (unsigned long long)d - 1) / (unsigned long long)d;
+}
+
+// ------------------------------------------------ asynchronous global->smem
+// cp.async (sm_80+ LDGSTS): the copy lands in shared memory without passing
+// through registers, so the next transform's input streams in while the
+// current one computes.  Both addresses are element aligned (8 or 16 bytes).
+template <typename V> __device__ __forceinline__ void cp_async_elem(V* sdst, const V* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (sizeof(V) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ----------------------------------------------------- Stockham radix pass
 // One pass over Gw sub-transforms of length L held in smem: element i of
 // sub-transform g lives at buf[g*gs + i*is].  s = product of earlier radices.
-template <typename V, int EMAX, int R>
-__device__ __noinline__ void spass(V* __restrict__ buf, int L, int Gw, int is, int gs, int s,
+// The team is the whole block (WARP = false) or one warp that owns these
+// sub-transforms alone (WARP = true, synchronised with __syncwarp).
+// Work item w = b*Gw + g (g fastest: adjacent threads touch adjacent
+// sub-transforms), butterfly b = pp*s + q; the items of one thread are
+// enumerated with carries instead of divisions.
+template <typename V, int EMAX, int R, bool WARP>
+__device__ __forceinline__ void spass(V* __restrict__ buf, int L, int Gw, int is, int gs, int s,
                                       const V* __restrict__ tw) {
     constexpr int SL = EMAX / R;
-    const int T = blockDim.x, tid = threadIdx.x;
+    const int T = WARP ? 32 : (int)blockDim.x;
+    const int tid = WARP ? (opaque_tid() & 31) : opaque_tid();
     const int nb = L / R;
     const int W = Gw * nb;
     V v[SL][R];
     int off[SL], pp_[SL];
+    int g = tid % Gw, b = tid / Gw;
+    int pp = b / s, q = b - pp * s;
+    const int dg = T % Gw, db = T / Gw;
+    const int dpp = db / s, dq = db - dpp * s;
 #pragma unroll
     for (int i = 0; i < SL; i++) {
         const int w = tid + i * T;
         off[i] = -1;
         if (w < W) {
-            const int g = w % Gw, b = w / Gw;
-            const int pp = b / s, q = b - pp * s;
             const V* src = buf + g * gs + (q + s * pp) * is;
 #pragma unroll
             for (int k = 0; k < R; k++) v[i][k] = src[k * nb * is];
             off[i] = g * gs + (q + s * R * pp) * is;
             pp_[i] = pp;
         }
+        // advance (g, b) by T and (pp, q) by the resulting change of b
+        g += dg;
+        int carry = 0;
+        if (g >= Gw) { g -= Gw; carry = 1; }
+        q += dq + carry;
+        pp += dpp;
+        if (q >= s) { q -= s; pp += 1; }
     }
-    __syncthreads();
+    if (WARP) __syncwarp(); else __syncthreads();
 #pragma unroll
     for (int i = 0; i < SL; i++) {
         if (off[i] >= 0) {
             dft<R>(v[i]);
-            const int pp = pp_[i];
-            if (pp) {
+            const int p0 = pp_[i];
+            if (p0) {
 #pragma unroll
-                for (int j = 1; j < R; j++) v[i][j] = cmul(v[i][j], __ldg(tw + j * pp * s));
+                for (int j = 1; j < R; j++) v[i][j] = cmul(v[i][j], tw[j * p0 * s]);
             }
             V* dst = buf + off[i];
 #pragma unroll
             for (int j = 0; j < R; j++) dst[j * s * is] = v[i][j];
         }
     }
-    __syncthreads();
+    if (WARP) __syncwarp(); else __syncthreads();
 }
 
-// All passes of `count` sub-transforms, in waves of P.G.  Caller must have
-// synchronised the block after writing buf; returns synchronised.
-template <typename V, int EMAX>
-__device__ __forceinline__ void run_subffts(V* buf, const SubPlan& P, int count, int is, int gs) {
-    const V* tw = (const V*)P.tw;
-    for (int g0 = 0; g0 < count; g0 += P.G) {
-        const int Gw = min(P.G, count - g0);
-        V* b = buf + g0 * gs;
-        int s = 1;
-        for (int q = 0; q < P.np; q++) {
-            const int r = P.radix[q];
-            switch (r) {
-                case 2: spass<V, EMAX, 2>(b, P.L, Gw, is, gs, s, tw); break;
-                case 3: spass<V, EMAX, 3>(b, P.L, Gw, is, gs, s, tw); break;
-                case 4: spass<V, EMAX, 4>(b, P.L, Gw, is, gs, s, tw); break;
-                case 5: spass<V, EMAX, 5>(b, P.L, Gw, is, gs, s, tw); break;
-                case 7: spass<V, EMAX, 7>(b, P.L, Gw, is, gs, s, tw); break;
-                case 8: spass<V, EMAX, 8>(b, P.L, Gw, is, gs, s, tw); break;
-                case 9: spass<V, EMAX, 9>(b, P.L, Gw, is, gs, s, tw); break;
-                case 16: spass<V, EMAX, 16>(b, P.L, Gw, is, gs, s, tw); break;
-                default: break;
-            }
-            s *= r;
+// All passes of `count` sub-transforms, pass-major.  The radix sequence is
+// canonical -- 16^a 9^b 8^c 7^d 5^e 4^f 3^g 2^h, multiplicities in P.cnt[] --
+// and runs as eight fixed-radix loops with runtime trip counts: every pass
+// body is a compile-time radix, so no runtime switch widens the register live
+// ranges (a switch over radices spills FP64 codelets).
+// Block mode: waves of P.G whole sub-transforms (disjoint element sets, so
+// each wave's read-barrier-write is a complete in-place pass).
+// Warp mode (P.Gwarp > 0): warp w owns groups of P.Gwarp sub-transforms
+// (w, w + nwarps, ...) and never waits for the other warps.
+// Caller must have synchronised the block after writing buf; returns
+// synchronised.
+template <typename V, int EMAX, int R>
+__device__ __forceinline__ void radix_loop(V* buf, const SubPlan& P, int count, int is, int gs, int& s,
+                                           const V* tw, int cnt) {
+    if (P.Gwarp > 0) {
+        const int nw = blockDim.x >> 5, wid = opaque_tid() >> 5;
+        const int step = nw * P.Gwarp;
+        for (int i = 0; i < cnt; i++) {
+            for (int g0 = wid * P.Gwarp; g0 < count; g0 += step)
+                spass<V, EMAX, R, true>(buf + g0 * gs, P.L, min(P.Gwarp, count - g0), is, gs, s, tw);
+            s *= R;
+        }
+    } else {
+        for (int i = 0; i < cnt; i++) {
+            for (int g0 = 0; g0 < count; g0 += P.G)
+                spass<V, EMAX, R, false>(buf + g0 * gs, P.L, min(P.G, count - g0), is, gs, s, tw);
+            s *= R;
         }
     }
+}
+template <typename V, int EMAX>
+__device__ __forceinline__ void run_subffts(V* buf, const SubPlan& P, const V* tw, int count, int is,
+                                            int gs) {
+    int s = 1;
+    radix_loop<V, EMAX, 16>(buf, P, count, is, gs, s, tw, P.cnt[0]);
+    radix_loop<V, EMAX, 9>(buf, P, count, is, gs, s, tw, P.cnt[1]);
+    radix_loop<V, EMAX, 8>(buf, P, count, is, gs, s, tw, P.cnt[2]);
+    radix_loop<V, EMAX, 7>(buf, P, count, is, gs, s, tw, P.cnt[3]);
+    radix_loop<V, EMAX, 5>(buf, P, count, is, gs, s, tw, P.cnt[4]);
+    radix_loop<V, EMAX, 4>(buf, P, count, is, gs, s, tw, P.cnt[5]);
+    radix_loop<V, EMAX, 3>(buf, P, count, is, gs, s, tw, P.cnt[6]);
+    radix_loop<V, EMAX, 2>(buf, P, count, is, gs, s, tw, P.cnt[7]);
+    if (P.Gwarp > 0) __syncthreads();
+}
+template <typename V, int EMAX>
+__device__ __forceinline__ void run_subffts(V* buf, const SubPlan& P, int count, int is, int gs) {
+    run_subffts<V, EMAX>(buf, P, (const V*)P.tw, count, is, gs);
 }
 
 // block-wide FP64 complex sum (result valid in every thread)
@@ -166,7 +236,7 @@ __device__ __forceinline__ double2 block_sum(double2 v, double2* scratch) {
         v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
         v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
     }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = opaque_tid() & 31, wid = opaque_tid() >> 5, nw = blockDim.x >> 5;
     __syncthreads();
     if (lane == 0) scratch[wid] = v;
     __syncthreads();
@@ -180,7 +250,7 @@ __device__ __forceinline__ double2 block_sum(double2 v, double2* scratch) {
 // smem: buf[V][PC] (+ for Rader: xs[V][XP]) + reduction scratch
 template <typename V, int EMAX>
 __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem) {
-    const int T = blockDim.x, tid = threadIdx.x;
+    const int T = blockDim.x, tid = opaque_tid();
     V* buf = (V*)smem;
     V* xs = buf + (size_t)p.V * p.PC;
     const int t0 = blockIdx.x * p.V;
@@ -192,13 +262,13 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
 
     if (p.conv == CONV_NONE) {
         for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = idx / nx, i = idx - r * nx;
+            const int r = fdiv(idx, p.mX), i = idx - r * nx;
             buf[r * p.PC + i] = load_in(p, ldg_stream(in + (long long)r * p.in_dist + i));
         }
         __syncthreads();
         run_subffts<V, EMAX>(buf, p.pc, nrows, 1, p.PC);
         for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = idx / nx, i = idx - r * nx;
+            const int r = fdiv(idx, p.mX), i = idx - r * nx;
             stg_stream(out + (long long)r * p.out_dist + i, store_out(p, buf[r * p.PC + i]));
         }
         return;
@@ -206,18 +276,18 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
 
     if (p.conv == CONV_RADER) {
         for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = idx / nx, i = idx - r * nx;
+            const int r = fdiv(idx, p.mX), i = idx - r * nx;
             xs[r * p.XP + i] = load_in(p, ldg_stream(in + (long long)r * p.in_dist + i));
         }
         __syncthreads();
         const int L = nx - 1;
         for (int idx = tid; idx < nrows * M; idx += T) {
-            const int r = idx / M, j = idx - r * M;
+            const int r = fdiv(idx, p.mM), j = idx - r * M;
             buf[r * p.PC + j] = (j < L) ? xs[r * p.XP + __ldg(p.perm + j)] : zero<V>();
         }
     } else {
         for (int idx = tid; idx < nrows * M; idx += T) {
-            const int r = idx / M, j = idx - r * M;
+            const int r = fdiv(idx, p.mM), j = idx - r * M;
             V v = zero<V>();
             if (j < nx) {
                 V x = load_in(p, ldg_stream(in + (long long)r * p.in_dist + j));
@@ -229,7 +299,7 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
     __syncthreads();
     run_subffts<V, EMAX>(buf, p.pc, nrows, 1, p.PC);
     for (int idx = tid; idx < nrows * M; idx += T) {
-        const int r = idx / M, k = idx - r * M;
+        const int r = fdiv(idx, p.mM), k = idx - r * M;
         V* e = buf + r * p.PC + k;
         *e = conjv(fromd<V>(cmul(tod(*e), __ldg(p.spec + k))));
     }
@@ -240,7 +310,7 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
         const int L = nx - 1;
         // y[g^-j] = x0 + c[j]  (prime.jl:76-78), written into the staging rows
         for (int idx = tid; idx < nrows * L; idx += T) {
-            const int r = idx / L, j = idx - r * L;
+            const int r = fdiv(idx, p.mL), j = idx - r * L;
             const V x0 = xs[r * p.XP];
             const V c = conjv(buf[r * p.PC + j]);
             buf[r * p.PC + j] = mk<V>(x0.x + c.x, x0.y + c.y);  // park result in place
@@ -262,17 +332,17 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
         }
         __syncthreads();
         for (int idx = tid; idx < nrows * L; idx += T) {
-            const int r = idx / L, j = idx - r * L;
+            const int r = fdiv(idx, p.mL), j = idx - r * L;
             xs[r * p.XP + __ldg(p.iperm + j)] = buf[r * p.PC + j];
         }
         __syncthreads();
         for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = idx / nx, i = idx - r * nx;
+            const int r = fdiv(idx, p.mX), i = idx - r * nx;
             stg_stream(out + (long long)r * p.out_dist + i, store_out(p, xs[r * p.XP + i]));
         }
     } else {
         for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = idx / nx, k = idx - r * nx;
+            const int r = fdiv(idx, p.mX), k = idx - r * nx;
             const V c = conjv(buf[r * p.PC + k]);
             const V y = fromd<V>(cmul(tod(c), __ldg(p.chirp + k)));
             stg_stream(out + (long long)r * p.out_dist + k, store_out(p, y));
@@ -283,118 +353,207 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
 // ---------------------------------------------------------------- FOUR mode
 // Column layout (step A): (i1, j) at i1*PA + j, j < W = N2/C
 // Row layout    (step C): (r, i2) at r*PC + i2, r < N1/C
-template <typename V, int EMAX>
-__device__ __forceinline__ void four_exchange_fwd(const KParams& p, V* buf, cg::cluster_group& cl, unsigned c) {
-    // row (r, i2) <- column buffer of CTA i2/W at (k1, i2 % W), times w^(i2 k1)
-    const int C = p.C, W = p.N2 / C, R1 = p.N1 / C;
-    const int T = blockDim.x, tid = threadIdx.x;
-    const int total = R1 * p.N2;
-    V v[EMAX];
-    cl.sync();
-#pragma unroll
-    for (int i = 0; i < EMAX; i++) {
-        const int idx = tid + i * T;
-        if (idx < total) {
-            const int r = idx / p.N2, i2 = idx - r * p.N2;
-            const int k1 = c * R1 + r, owner = i2 / W;
-            const V* rb = cl.map_shared_rank(buf, owner);
-            v[i] = apply_tw(rb[k1 * p.PA + (i2 - owner * W)], p.t4, (unsigned)(i2 * k1));
-        }
+//
+// The body is written once against a shape policy K: DynK reads the shape
+// from KParams (any size the planner picks), StatK<...> fixes it at compile
+// time for the hot sizes so strides, counts and divisions fold to constants.
+struct DynK {
+    __device__ static int N1(const KParams& p) { return p.N1; }
+    __device__ static int N2(const KParams& p) { return p.N2; }
+    __device__ static int C(const KParams& p) { return p.C; }
+    __device__ static int PA(const KParams& p) { return p.PA; }
+    __device__ static int PC(const KParams& p) { return p.PC; }
+    __device__ static int W(const KParams& p) { return p.N2 / p.C; }
+    __device__ static int R1(const KParams& p) { return p.N1 / p.C; }
+    __device__ static int dW(const KParams& p, unsigned x) { return fdiv(x, p.mW); }
+    __device__ static int dN2(const KParams& p, unsigned x) { return fdiv(x, p.mN2); }
+    __device__ static int dR1(const KParams& p, unsigned x) { return fdiv(x, p.mR1); }
+    template <typename V, int EMAX> __device__ static void colA(V* buf, const KParams& p, const V* tw) {
+        run_subffts<V, EMAX>(buf, p.pa, tw, p.N2 / p.C, p.PA, 1);
     }
-    cl.sync();
-#pragma unroll
-    for (int i = 0; i < EMAX; i++) {
-        const int idx = tid + i * T;
-        if (idx < total) {
-            const int r = idx / p.N2, i2 = idx - r * p.N2;
-            buf[r * p.PC + i2] = v[i];
-        }
+    template <typename V, int EMAX> __device__ static void rowC(V* buf, const KParams& p, const V* tw) {
+        run_subffts<V, EMAX>(buf, p.pc, tw, p.N1 / p.C, 1, p.PC);
     }
-    __syncthreads();
+};
+
+// compile-time radix sequence (canonical order) and its pass chain
+template <int... R> struct Seq {};
+template <typename V, int EMAX, bool WARP, int L, int IS, int GS, int COUNT, int GW, int S, int R,
+          int... Rest>
+__device__ __forceinline__ void st_passes(V* buf, const V* tw) {
+    if constexpr (WARP) {
+        const int nw = blockDim.x >> 5, wid = opaque_tid() >> 5;
+        for (int g0 = wid * GW; g0 < COUNT; g0 += nw * GW) {
+            if constexpr (COUNT % GW == 0)
+                spass<V, EMAX, R, true>(buf + g0 * GS, L, GW, IS, GS, S, tw);
+            else
+                spass<V, EMAX, R, true>(buf + g0 * GS, L, min(GW, COUNT - g0), IS, GS, S, tw);
+        }
+    } else {
+#pragma unroll
+        for (int g0 = 0; g0 < COUNT; g0 += GW)
+            spass<V, EMAX, R, false>(buf + g0 * GS, L, (COUNT - g0 < GW) ? COUNT - g0 : GW, IS, GS, S, tw);
+    }
+    if constexpr (sizeof...(Rest) > 0)
+        st_passes<V, EMAX, WARP, L, IS, GS, COUNT, GW, S * R, Rest...>(buf, tw);
+}
+template <typename V, int EMAX, bool WARP, int L, int IS, int GS, int COUNT, int GW, int... R>
+__device__ __forceinline__ void st_subffts(V* buf, const V* tw, Seq<R...>) {
+    st_passes<V, EMAX, WARP, L, IS, GS, COUNT, GW, 1, R...>(buf, tw);
+    if constexpr (WARP) __syncthreads();
 }
 
-template <typename V, int EMAX>
-__device__ __forceinline__ void four_exchange_inv(const KParams& p, V* buf, cg::cluster_group& cl, unsigned c) {
-    // column (k1, j) <- row buffer of CTA k1/R1 at (k1 % R1, c*W + j), times w^(i2 k1)
-    const int C = p.C, W = p.N2 / C, R1 = p.N1 / C;
-    const int T = blockDim.x, tid = threadIdx.x;
-    const int total = p.N1 * W;
-    V v[EMAX];
-    cl.sync();
-#pragma unroll
-    for (int i = 0; i < EMAX; i++) {
-        const int idx = tid + i * T;
-        if (idx < total) {
-            const int k1 = idx / W, j = idx - k1 * W;
-            const int owner = k1 / R1, i2 = c * W + j;
-            const V* rb = cl.map_shared_rank(buf, owner);
-            v[i] = apply_tw(rb[(k1 - owner * R1) * p.PC + i2], p.t4, (unsigned)(i2 * k1));
-        }
+template <int N1_, int N2_, int C_, class SA, bool WA, int GA, class SC, bool WC, int GC>
+struct StatK {
+    static constexpr int kW = N2_ / C_, kR1 = N1_ / C_;
+    static constexpr int kPC = N2_ + ((N2_ % 2 == 0) ? 1 : 0);
+    static constexpr int kPA = (C_ == 1) ? kPC : kW;
+    __device__ static constexpr int N1(const KParams&) { return N1_; }
+    __device__ static constexpr int N2(const KParams&) { return N2_; }
+    __device__ static constexpr int C(const KParams&) { return C_; }
+    __device__ static constexpr int PA(const KParams&) { return kPA; }
+    __device__ static constexpr int PC(const KParams&) { return kPC; }
+    __device__ static constexpr int W(const KParams&) { return kW; }
+    __device__ static constexpr int R1(const KParams&) { return kR1; }
+    __device__ static int dW(const KParams&, unsigned x) { return (int)(x / (unsigned)kW); }
+    __device__ static int dN2(const KParams&, unsigned x) { return (int)(x / (unsigned)N2_); }
+    __device__ static int dR1(const KParams&, unsigned x) { return (int)(x / (unsigned)kR1); }
+    template <typename V, int EMAX> __device__ static void colA(V* buf, const KParams&, const V* tw) {
+        st_subffts<V, EMAX, WA, N1_, kPA, 1, kW, GA>(buf, tw, SA{});
+    }
+    template <typename V, int EMAX> __device__ static void rowC(V* buf, const KParams&, const V* tw) {
+        st_subffts<V, EMAX, WC, N2_, 1, kPC, kR1, GC>(buf, tw, SC{});
+    }
+};
+
+// Exchanges between the column and row layouts, push style: every CTA
+// multiplies its own elements by the four-step twiddle and stores them into
+// the owning peer's buffer through distributed shared memory (stores do not
+// wait for a reply), then one cluster barrier publishes them.  The target
+// buffers are idle: bufC is first read after this barrier, and bufA is
+// written back only after the forward exchange's barrier, by which time
+// every CTA has finished reading its own bufA.
+template <typename V, class K>
+__device__ __forceinline__ void four_push_fwd(const KParams& p, const V* bufA, V* bufC,
+                                              cg::cluster_group& cl, unsigned c, const TwoLevel& t4) {
+    // (k1, j) of this CTA's columns -> CTA k1/R1, row k1 % R1, column i2 = c*W + j
+    const int W = K::W(p), R1 = K::R1(p), PA = K::PA(p), PC = K::PC(p);
+    const int T = blockDim.x, tid = opaque_tid();
+    const int total = K::N1(p) * W;
+    for (int idx = tid; idx < total; idx += T) {
+        const int k1 = K::dW(p, idx), j = idx - k1 * W;
+        const int i2 = c * W + j, d = K::dR1(p, k1);
+        V* dst = cl.map_shared_rank(bufC, d);
+        dst[(k1 - d * R1) * PC + i2] = apply_tw(bufA[k1 * PA + j], t4, (unsigned)(i2 * k1));
     }
     cl.sync();
-#pragma unroll
-    for (int i = 0; i < EMAX; i++) {
-        const int idx = tid + i * T;
-        if (idx < total) {
-            const int k1 = idx / W, j = idx - k1 * W;
-            buf[k1 * p.PA + j] = v[i];
-        }
+}
+template <typename V, class K>
+__device__ __forceinline__ void four_push_inv(const KParams& p, V* bufA, const V* bufC,
+                                              cg::cluster_group& cl, unsigned c, const TwoLevel& t4) {
+    // (r, i2) of this CTA's rows (k1 = c*R1 + r) -> CTA i2/W, column i2 % W, row k1
+    const int W = K::W(p), R1 = K::R1(p), N2 = K::N2(p), PA = K::PA(p), PC = K::PC(p);
+    const int T = blockDim.x, tid = opaque_tid();
+    const int total = R1 * N2;
+    for (int idx = tid; idx < total; idx += T) {
+        const int r = K::dN2(p, idx), i2 = idx - r * N2;
+        const int k1 = c * R1 + r, d = K::dW(p, i2);
+        V* dst = cl.map_shared_rank(bufA, d);
+        dst[k1 * PA + (i2 - d * W)] = apply_tw(bufC[r * PC + i2], t4, (unsigned)(i2 * k1));
     }
-    __syncthreads();
+    cl.sync();
 }
 
 // single-CTA four-step: twiddle in place (PA == PC, same layout)
-template <typename V>
-__device__ __forceinline__ void four_twiddle_local(const KParams& p, V* buf) {
-    const int T = blockDim.x, tid = threadIdx.x;
-    for (int idx = tid; idx < p.M; idx += T) {
-        const int k1 = idx / p.N2, i2 = idx - k1 * p.N2;
-        V* e = buf + k1 * p.PA + i2;
-        *e = apply_tw(*e, p.t4, (unsigned)(i2 * k1));
+template <typename V, class K>
+__device__ __forceinline__ void four_twiddle_local(const KParams& p, V* buf, const TwoLevel& t4) {
+    const int T = blockDim.x, tid = opaque_tid();
+    const int N2 = K::N2(p), total = K::N1(p) * N2;
+    for (int idx = tid; idx < total; idx += T) {
+        const int k1 = K::dN2(p, idx), i2 = idx - k1 * N2;
+        V* e = buf + k1 * K::PA(p) + i2;
+        *e = apply_tw(*e, t4, (unsigned)(i2 * k1));
     }
     __syncthreads();
 }
 
-template <typename V, int EMAX>
-__device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem) {
-    cg::cluster_group cl = cg::this_cluster();
-    const int C = p.C;
-    const unsigned c = (C > 1) ? cl.block_rank() : 0;
-    const int t = blockIdx.x / C;
-    if (t >= p.batch) return;             // uniform across the cluster
-    const int T = blockDim.x, tid = threadIdx.x;
-    const int N1 = p.N1, N2 = p.N2, W = N2 / C, R1 = N1 / C, M = p.M, nx = p.nx;
-    const int bufsz = max(N1 * p.PA, R1 * p.PC);
-    V* buf = (V*)smem;
-    V* xs = buf + bufsz;                  // Rader x chunk (XP elements)
-    double2* red = after16(xs + p.XP);    // reduction scratch (32 + C entries)
+// Shared-memory carve-up of a FOUR CTA (host and device agree on it):
+//   twA[N1] twC[N2] (V)  t4lo[2^bits] t4hi[nhi] (FP64)  bufA[N1*PA]
+//   bufC[R1*PC] (C > 1 only; C = 1 works in place)  xs[XP] (Rader)
+//   red[48] (FP64, 16-byte aligned)
+// One transform per cluster.  The CTA first issues cp.async copies of its
+// input slice (they land in shared memory without passing through
+// registers), stages the twiddle tables while those are in flight, then
+// computes.  A persistent loop over transforms would let the next input
+// stream in during compute, but any loop around this body makes the
+// compiler keep per-thread index state live across it and the FP64
+// codelets spill; two co-resident CTAs per SM provide the overlap instead.
+template <typename V, class K>
+__device__ __forceinline__ void four_prefetch(const KParams& p, V* dst, int t, unsigned c) {
+    const int T = blockDim.x, tid = opaque_tid();
     const V* in = (const V*)p.in + (long long)t * p.in_dist;
-    V* out = (V*)p.out + (long long)t * p.out_dist;
+    if (p.conv == CONV_RADER) {
+        const int XC = p.XP;                      // staging of this CTA's x chunk
+        for (int i = tid; i < XC; i += T) {
+            const int gi = c * XC + i;
+            if (gi < p.nx) cp_async_elem(dst + i, in + gi);
+        }
+    } else {
+        const int N2 = K::N2(p), W = K::W(p), PA = K::PA(p), total = K::N1(p) * W;
+        const int lim = (p.conv == CONV_BLUE) ? p.nx : 0x7fffffff;
+        for (int idx = tid; idx < total; idx += T) {
+            const int i1 = K::dW(p, idx), j = idx - i1 * W;
+            const int jj = i1 * N2 + c * W + j;
+            if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
+        }
+    }
+    cp_async_commit();
+}
 
-    // ---- prologue: column layout of the (padded) input
+// One transform of the persistent FOUR loop.  The thread and CTA indices are
+// re-read through volatile asm on every call: otherwise the compiler hoists
+// every index expression derived from them out of the persistent loop and
+// the values it keeps live across the body push the FP64 codelets into
+// spills.
+template <typename V, int EMAX, class K>
+__device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC, V* nxt, V* xs, double2* red,
+                                            const V* twA, const V* twC, const TwoLevel& t4, int t,
+                                            int tn, unsigned c) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = K::C(p);
+    const int T = blockDim.x, tid = opaque_tid();
+    const int N1 = K::N1(p), N2 = K::N2(p), W = K::W(p), R1 = K::R1(p), nx = p.nx;
+    const int PA = K::PA(p), PC = K::PC(p);
+    V* out = (V*)p.out + (long long)t * p.out_dist;
+    cp_async_wait_all();
+    __syncthreads();
+
+    // ---- prologue fix-ups on the arrived input (column layout)
     double2 xsum = make_double2(0, 0);
     V x0 = zero<V>();
     if (p.conv == CONV_NONE) {
-        for (int idx = tid; idx < N1 * W; idx += T) {
-            const int i1 = idx / W, j = idx - i1 * W;
-            buf[i1 * p.PA + j] = load_in(p, ldg_stream(in + (long long)i1 * N2 + c * W + j));
+        if (p.dir) {
+            for (int idx = tid; idx < N1 * W; idx += T) {
+                const int i1 = K::dW(p, idx), j = idx - i1 * W;
+                V* e = buf + i1 * PA + j;
+                *e = conjv(*e);
+            }
         }
     } else if (p.conv == CONV_BLUE) {
         for (int idx = tid; idx < N1 * W; idx += T) {
-            const int i1 = idx / W, j = idx - i1 * W;
+            const int i1 = K::dW(p, idx), j = idx - i1 * W;
             const int jj = i1 * N2 + c * W + j;
-            V v = zero<V>();
-            if (jj < nx) v = fromd<V>(cmul(tod(load_in(p, ldg_stream(in + jj))), __ldg(p.chirp + jj)));
-            buf[i1 * p.PA + j] = v;
+            V* e = buf + i1 * PA + j;
+            *e = (jj < nx) ? fromd<V>(cmul(tod(load_in(p, *e)), __ldg(p.chirp + jj))) : zero<V>();
         }
     } else {
-        // stage x in distributed chunks, sum x[1:], gather a[j] = x[g^j]
+        // x chunk staged at buf[0..XC): conj, sum x[1:], publish to xs
         const int XC = p.XP;
         double2 acc = make_double2(0, 0);
         for (int i = tid; i < XC; i += T) {
             const int gi = c * XC + i;
             V v = zero<V>();
-            if (gi < nx) v = load_in(p, ldg_stream(in + gi));
+            if (gi < nx) v = load_in(p, buf[i]);
             xs[i] = v;
             if (gi >= 1 && gi < nx) { double2 d = tod(v); acc.x += d.x; acc.y += d.y; }
         }
@@ -411,56 +570,59 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
         }
         const int L = nx - 1;
         for (int idx = tid; idx < N1 * W; idx += T) {
-            const int i1 = idx / W, j = idx - i1 * W;
+            const int i1 = K::dW(p, idx), j = idx - i1 * W;
             const int jj = i1 * N2 + c * W + j;
             V v = zero<V>();
             if (jj < L) {
-                const int src = __ldg(p.perm + jj), owner = src / XC;
+                const int src = __ldg(p.perm + jj), owner = fdiv(src, p.mX);
                 const V* rx = (C > 1) ? cl.map_shared_rank(xs, owner) : xs;
                 v = rx[src - owner * XC];
             }
-            buf[i1 * p.PA + j] = v;
+            buf[i1 * PA + j] = v;
         }
     }
     __syncthreads();
+    // the idle buffer is free: nobody reads it any more (its last remote
+    // reader passed the previous transform's exchange barrier)
+    if (tn >= 0) four_prefetch<V, K>(p, nxt, tn, c);
 
-    // ---- forward FFT_M: columns, twiddle + exchange, rows
-    run_subffts<V, EMAX>(buf, p.pa, W, p.PA, 1);
-    if (C > 1) four_exchange_fwd<V, EMAX>(p, buf, cl, c);
-    else four_twiddle_local(p, buf);
-    run_subffts<V, EMAX>(buf, p.pc, R1, 1, p.PC);
+    // ---- forward FFT_M: columns, twiddle + exchange, rows (buf = column layout)
+    K::template colA<V, EMAX>(buf, p, twA);
+    if (C > 1) four_push_fwd<V, K>(p, buf, bufC, cl, c, t4);
+    else four_twiddle_local<V, K>(p, buf, t4);
+    K::template rowC<V, EMAX>(bufC, p, twC);
 
     if (p.conv == CONV_NONE) {
         // X[k1 + N1 k2] from row layout (r, k2), k1 = c*R1 + r
         for (int idx = tid; idx < R1 * N2; idx += T) {
-            const int k2 = idx / R1, r = idx - k2 * R1;
+            const int k2 = K::dR1(p, idx), r = idx - k2 * R1;
             stg_stream(out + (long long)(c * R1 + r) + (long long)N1 * k2,
-                       store_out(p, buf[r * p.PC + k2]));
+                       store_out(p, bufC[r * PC + k2]));
         }
         return;
     }
 
     // ---- pointwise multiply by spectrum/M and conjugate (inverse via conj)
     for (int idx = tid; idx < R1 * N2; idx += T) {
-        const int r = idx / N2, k2 = idx - r * N2;
-        const int k = (c * R1 + r) + N1 * k2;
-        V* e = buf + r * p.PC + k2;
-        *e = conjv(fromd<V>(cmul(tod(*e), __ldg(p.spec + k))));
+        const int r = K::dN2(p, idx), k2 = idx - r * N2;
+        const int kk = (c * R1 + r) + N1 * k2;
+        V* e = bufC + r * PC + k2;
+        *e = conjv(fromd<V>(cmul(tod(*e), __ldg(p.spec + kk))));
     }
     __syncthreads();
     // ---- second FFT_M in transposed order: rows, twiddle + exchange, columns
-    run_subffts<V, EMAX>(buf, p.pc, R1, 1, p.PC);
-    if (C > 1) four_exchange_inv<V, EMAX>(p, buf, cl, c);
-    else four_twiddle_local(p, buf);
-    run_subffts<V, EMAX>(buf, p.pa, W, p.PA, 1);
+    K::template rowC<V, EMAX>(bufC, p, twC);
+    if (C > 1) four_push_inv<V, K>(p, buf, bufC, cl, c, t4);
+    else four_twiddle_local<V, K>(p, buf, t4);
+    K::template colA<V, EMAX>(buf, p, twA);
     // column layout now holds conj(c[j1*N2 + c*W + j])
 
     if (p.conv == CONV_BLUE) {
         for (int idx = tid; idx < N1 * W; idx += T) {
-            const int j1 = idx / W, j = idx - j1 * W;
+            const int j1 = K::dW(p, idx), j = idx - j1 * W;
             const int jj = j1 * N2 + c * W + j;
             if (jj < nx) {
-                const V cv = conjv(buf[j1 * p.PA + j]);
+                const V cv = conjv(buf[j1 * PA + j]);
                 stg_stream(out + jj, store_out(p, fromd<V>(cmul(tod(cv), __ldg(p.chirp + jj)))));
             }
         }
@@ -471,11 +633,11 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
     const int XC = p.XP, L = nx - 1;
     if (C > 1) cl.sync(); else __syncthreads();   // everyone done reading xs
     for (int idx = tid; idx < N1 * W; idx += T) {
-        const int j1 = idx / W, j = idx - j1 * W;
+        const int j1 = K::dW(p, idx), j = idx - j1 * W;
         const int jj = j1 * N2 + c * W + j;
         if (jj < L) {
-            const V cv = conjv(buf[j1 * p.PA + j]);
-            const int dst = __ldg(p.iperm + jj), owner = dst / XC;
+            const V cv = conjv(buf[j1 * PA + j]);
+            const int dst = __ldg(p.iperm + jj), owner = fdiv(dst, p.mX);
             V* rx = (C > 1) ? cl.map_shared_rank(xs, owner) : xs;
             rx[dst - owner * XC] = mk<V>(x0.x + cv.x, x0.y + cv.y);
         }
@@ -490,7 +652,42 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
         const int gi = c * XC + i;
         if (gi < nx) stg_stream(out + gi, store_out(p, xs[i]));
     }
-    if (C > 1) cl.sync();                          // keep smem alive for peers
+    // xs is rewritten by the next transform's prologue only after a
+    // cluster barrier, so no extra barrier is needed here
+    __syncthreads();
+}
+
+template <typename V, int EMAX, class K>
+__device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem) {
+    const int C = K::C(p);
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned c = (C > 1) ? cl.block_rank() : 0;
+    const int t = blockIdx.x / C;
+    if (t >= p.batch) return;             // uniform across the cluster
+    const int T = blockDim.x, tid = opaque_tid();
+    const int N1 = K::N1(p), N2 = K::N2(p);
+    const int nlo = 1 << p.t4.bits, nhi = (p.t4.N + nlo - 1) / nlo + 1;
+
+    V* twA = (V*)smem;
+    V* twC = twA + N1;
+    double2* t4lo = after16(twC + N2);
+    double2* t4hi = t4lo + nlo;
+    V* buf = (V*)(t4hi + nhi);            // column layout (N1 x PA)
+    V* bufC = (C > 1) ? buf + N1 * K::PA(p) : buf;   // row layout (R1 x PC)
+    V* xs = (C > 1) ? bufC + K::R1(p) * K::PC(p) : buf + N1 * K::PA(p);  // Rader x chunk
+    double2* red = after16(xs + p.XP);    // reduction scratch (32 + C entries)
+
+    four_prefetch<V, K>(p, buf, t, c);
+    // tables -> shared memory while the input is in flight
+    for (int i = tid; i < N1; i += T) twA[i] = ((const V*)p.pa.tw)[i];
+    for (int i = tid; i < N2; i += T) twC[i] = ((const V*)p.pc.tw)[i];
+    for (int i = tid; i < nlo; i += T) t4lo[i] = p.t4.lo[i];
+    for (int i = tid; i < nhi; i += T) t4hi[i] = p.t4.hi[i];
+    TwoLevel t4 = p.t4;
+    t4.lo = t4lo;
+    t4.hi = t4hi;
+    four_transform<V, EMAX, K>(p, buf, bufC, nullptr, xs, red, twA, twC, t4, t, -1, c);
+    if (C > 1) cl.sync();                 // keep smem alive for peers
 }
 
 // ------------------------------------------------------- COLPASS / ROWPASS
@@ -498,7 +695,7 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
 // transform; column FFTs; store w^(i2 k1)-scaled result to scratch row-major.
 template <typename V, int EMAX>
 __device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* smem) {
-    const int T = blockDim.x, tid = threadIdx.x;
+    const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V;
     const int t = blockIdx.x / tiles, c0 = (blockIdx.x - t * tiles) * p.V;
     if (t >= p.batch) return;
@@ -507,7 +704,7 @@ __device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* sm
     V* out = (V*)p.out + (long long)t * p.out_dist;
     const int N1 = p.N1, N2 = p.N2, Vw = p.V;
     for (int idx = tid; idx < N1 * Vw; idx += T) {
-        const int i1 = idx / Vw, j = idx - i1 * Vw;
+        const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
         const long long jj = (long long)i1 * N2 + c0 + j;
         V v;
         if (p.pre == PRE_CHIRP) {
@@ -523,7 +720,7 @@ __device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* sm
     __syncthreads();
     run_subffts<V, EMAX>(buf, p.pa, Vw, p.PA, 1);
     for (int idx = tid; idx < N1 * Vw; idx += T) {
-        const int k1 = idx / Vw, j = idx - k1 * Vw;
+        const int k1 = fdiv(idx, p.mV), j = idx - k1 * Vw;
         const unsigned e = (unsigned)((unsigned long long)(c0 + j) * k1 % (unsigned long long)p.M);
         out[(long long)k1 * N2 + c0 + j] = apply_tw(buf[k1 * p.PA + j], p.t4, e);
     }
@@ -533,7 +730,7 @@ __device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* sm
 // X[k1 + N1 k2] (natural order), optionally with the Bluestein epilogue.
 template <typename V, int EMAX>
 __device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* smem) {
-    const int T = blockDim.x, tid = threadIdx.x;
+    const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N1 / p.V;
     const int t = blockIdx.x / tiles, r0 = (blockIdx.x - t * tiles) * p.V;
     if (t >= p.batch) return;
@@ -542,13 +739,13 @@ __device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* sm
     V* out = (V*)p.out + (long long)t * p.out_dist;
     const int N1 = p.N1, N2 = p.N2, Vw = p.V;
     for (int idx = tid; idx < Vw * N2; idx += T) {
-        const int r = idx / N2, i2 = idx - r * N2;
+        const int r = fdiv(idx, p.mN2), i2 = idx - r * N2;
         buf[r * p.PC + i2] = in[(long long)(r0 + r) * N2 + i2];
     }
     __syncthreads();
     run_subffts<V, EMAX>(buf, p.pc, Vw, 1, p.PC);
     for (int idx = tid; idx < Vw * N2; idx += T) {
-        const int k2 = idx / Vw, r = idx - k2 * Vw;
+        const int k2 = fdiv(idx, p.mV), r = idx - k2 * Vw;
         const long long k = (long long)(r0 + r) + (long long)N1 * k2;
         V v = buf[r * p.PC + k2];
         if (p.post == POST_CHIRP) {

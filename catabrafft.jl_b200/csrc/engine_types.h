@@ -7,8 +7,10 @@
 struct SubPlan {
     int L;                        // sub-transform length
     int np;                       // number of radix passes
-    int G;                        // sub-transforms per wave (fits EMAX regs/thread)
-    unsigned char radix[CFFT_MAXP];
+    int G;                        // sub-transforms per block-wide wave (fits EMAX regs/thread)
+    int Gwarp;                    // sub-transforms per warp group (0: block mode)
+    unsigned char radix[CFFT_MAXP];  // pass radices in execution order (canonical)
+    unsigned char cnt[8];         // multiplicities of 16, 9, 8, 7, 5, 4, 3, 2
     const void* tw;               // w_L^m, m < L, element type of the data
 };
 
@@ -46,5 +48,7 @@ struct KParams {
     int units;                    // CTAs (ROWS/FOUR clusters) or tiles per transform
     int dir;                      // 0 forward, 1 inverse (scaled), 2 backward
     double scale;                 // 1/nx for dir 1, else 1
+    // multiply-shift reciprocals (see fdiv) of the layout's divisors
+    unsigned long long mW, mN2, mR1, mX, mM, mL, mV;
 };
 

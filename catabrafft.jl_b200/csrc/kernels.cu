@@ -1,10 +1,11 @@
-// kernels.cu -- sm_100a kernel entry points and their launcher.
+// kernels.cu -- sm_100a kernel entry points, the registry of statically
+// shaped kernels, and the launcher.
 #include "engine.cuh"
 #include "kernels.h"
 
 // 256 threads per CTA; FP64 data keeps 2 CTAs/SM resident (128 regs/thread),
-// FP32 data 3 CTAs/SM (85 regs/thread).
-template <typename V> struct MinBlocks { static constexpr int value = 3; };
+// and so does FP32 data (the exchange staging needs the headroom).
+template <typename V> struct MinBlocks { static constexpr int value = 2; };
 template <> struct MinBlocks<double2> { static constexpr int value = 2; };
 
 template <typename V, int EMAX>
@@ -12,10 +13,10 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_rows(KPar
     extern __shared__ __align__(16) unsigned char smem[];
     rows_body<V, EMAX>(p, smem);
 }
-template <typename V, int EMAX>
+template <typename V, int EMAX, class K>
 __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_four(KParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
-    four_body<V, EMAX>(p, smem);
+    four_body<V, EMAX, K>(p, smem);
 }
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_colpass(KParams p) {
@@ -28,18 +29,18 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_rowpass(K
     rowpass_body<V, EMAX>(p, smem);
 }
 
-static const void* kernel_for(int mode, int dtype) {
+const void* cfft_kernel_for(int mode, int dtype) {
     if (dtype == CFFT_DT_C128) {
         switch (mode) {
             case MODE_ROWS: return (const void*)k_rows<double2, CFFT_EMAX>;
-            case MODE_FOUR: return (const void*)k_four<double2, CFFT_EMAX>;
+            case MODE_FOUR: return (const void*)k_four<double2, CFFT_EMAX, DynK>;
             case MODE_COLPASS: return (const void*)k_colpass<double2, CFFT_EMAX>;
             case MODE_ROWPASS: return (const void*)k_rowpass<double2, CFFT_EMAX>;
         }
     } else {
         switch (mode) {
             case MODE_ROWS: return (const void*)k_rows<float2, CFFT_EMAX>;
-            case MODE_FOUR: return (const void*)k_four<float2, CFFT_EMAX>;
+            case MODE_FOUR: return (const void*)k_four<float2, CFFT_EMAX, DynK>;
             case MODE_COLPASS: return (const void*)k_colpass<float2, CFFT_EMAX>;
             case MODE_ROWPASS: return (const void*)k_rowpass<float2, CFFT_EMAX>;
         }
@@ -47,8 +48,45 @@ static const void* kernel_for(int mode, int dtype) {
     return nullptr;
 }
 
-cudaError_t cfft_prepare_kernel(int mode, int dtype, size_t smem, int cluster) {
-    const void* f = kernel_for(mode, dtype);
+// ---- statically shaped FOUR kernels for the hot lengths
+// radix multiplicities are listed in the canonical order 16, 9, 8, 7, 5, 4, 3, 2
+struct StaticFour {
+    int dtype, N1, N2, C;
+    unsigned char ca[8], cc[8];
+    const void* fn;
+};
+// 30240 = 168 x 180 on a 12-CTA cluster (ComplexF64 mixed-radix batch)
+using K_168x180_c12 = StatK<168, 180, 12, Seq<8, 7, 3>, true, 1, Seq<9, 5, 4>, true, 1>;
+// Rader M = 20160 = 168 x 120 on an 8-CTA cluster (primes 10007 .. 10081)
+using K_168x120_c8 = StatK<168, 120, 8, Seq<8, 7, 3>, true, 1, Seq<8, 5, 3>, true, 3>;
+// 65536 = 256 x 256 on a 16-CTA cluster (ComplexF32 precision form)
+using K_256x256_c16 = StatK<256, 256, 16, Seq<16, 16>, true, 2, Seq<16, 16>, true, 2>;
+
+static const StaticFour kStatic[] = {
+    {CFFT_DT_C128, 168, 180, 12, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 1, 0, 0, 1, 1, 0, 0},
+     (const void*)k_four<double2, CFFT_EMAX, K_168x180_c12>},
+    {CFFT_DT_C64, 168, 180, 12, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 1, 0, 0, 1, 1, 0, 0},
+     (const void*)k_four<float2, CFFT_EMAX, K_168x180_c12>},
+    {CFFT_DT_C128, 168, 120, 8, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 0, 1, 0, 1, 0, 1, 0},
+     (const void*)k_four<double2, CFFT_EMAX, K_168x120_c8>},
+    {CFFT_DT_C64, 168, 120, 8, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 0, 1, 0, 1, 0, 1, 0},
+     (const void*)k_four<float2, CFFT_EMAX, K_168x120_c8>},
+    {CFFT_DT_C64, 256, 256, 16, {2, 0, 0, 0, 0, 0, 0, 0}, {2, 0, 0, 0, 0, 0, 0, 0},
+     (const void*)k_four<float2, CFFT_EMAX, K_256x256_c16>},
+};
+
+const void* cfft_static_four(int dtype, int N1, int N2, int C, const unsigned char* ca,
+                             const unsigned char* cc) {
+    for (const auto& e : kStatic) {
+        if (e.dtype != dtype || e.N1 != N1 || e.N2 != N2 || e.C != C) continue;
+        bool same = true;
+        for (int i = 0; i < 8; i++) same = same && e.ca[i] == ca[i] && e.cc[i] == cc[i];
+        if (same) return e.fn;
+    }
+    return nullptr;
+}
+
+cudaError_t cfft_prepare_fn(const void* f, size_t smem, int cluster) {
     if (!f) return cudaErrorInvalidValue;
     // always the device maximum: a smaller value set for one plan would break
     // another plan that shares the kernel and needs more
@@ -62,9 +100,8 @@ cudaError_t cfft_prepare_kernel(int mode, int dtype, size_t smem, int cluster) {
     return cudaSuccess;
 }
 
-cudaError_t cfft_launch(const KParams& p, int dtype, unsigned grid, int threads, size_t smem,
-                        int cluster, cudaStream_t stream) {
-    const void* f = kernel_for(p.mode, dtype);
+cudaError_t cfft_launch_fn(const void* f, const KParams& p, unsigned grid, int threads, size_t smem,
+                           int cluster, cudaStream_t stream) {
     if (!f) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid, 1, 1);
@@ -84,9 +121,7 @@ cudaError_t cfft_launch(const KParams& p, int dtype, unsigned grid, int threads,
     return cudaLaunchKernelExC(&cfg, f, args);
 }
 
-cudaError_t cfft_max_active_clusters(int mode, int dtype, int threads, size_t smem, int cluster,
-                                     int* out) {
-    const void* f = kernel_for(mode, dtype);
+cudaError_t cfft_max_active_clusters_fn(const void* f, int threads, size_t smem, int cluster, int* out) {
     if (!f) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cluster, 1, 1);

@@ -11,8 +11,12 @@
 
 #include "engine_types.h"
 
-cudaError_t cfft_prepare_kernel(int mode, int dtype, size_t smem, int cluster);
-cudaError_t cfft_launch(const KParams& p, int dtype, unsigned grid, int threads, size_t smem,
-                        int cluster, cudaStream_t stream);
-cudaError_t cfft_max_active_clusters(int mode, int dtype, int threads, size_t smem, int cluster,
-                                     int* out);
+// generic kernel for a mode, or nullptr
+const void* cfft_kernel_for(int mode, int dtype);
+// statically shaped FOUR kernel matching (N1, N2, C, radix multiplicities), or nullptr
+const void* cfft_static_four(int dtype, int N1, int N2, int C, const unsigned char* ca,
+                             const unsigned char* cc);
+cudaError_t cfft_prepare_fn(const void* fn, size_t smem, int cluster);
+cudaError_t cfft_launch_fn(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
+                           int cluster, cudaStream_t stream);
+cudaError_t cfft_max_active_clusters_fn(const void* fn, int threads, size_t smem, int cluster, int* out);

@@ -101,6 +101,18 @@ static std::vector<int> radix_split(int64_t L, const int* order = kRadices, int 
     }
     return r;
 }
+static unsigned long long magic(int64_t d) {
+    // ceil(2^40 / d); exact floor(n/d) for n < 2^24, d <= 2^16 (see fdiv)
+    if (d < 1) d = 1;
+    return ((1ULL << 40) + (unsigned long long)d - 1) / (unsigned long long)d;
+}
+static void radix_counts(const std::vector<int>& rad, unsigned char* cnt) {
+    for (int ci = 0; ci < 8; ci++) {
+        int c = 0;
+        for (int r : rad) c += (r == kRadices[ci]);
+        cnt[ci] = (unsigned char)c;
+    }
+}
 static int wave_G(const std::vector<int>& rad, int64_t L, int T) {
     if (L <= 1) return 1 << 20;
     int64_t g = 1 << 20;
@@ -182,11 +194,13 @@ static double2 pow_by_squaring(double2 x, int64_t p) {
 // ---------------------------------------------------------------- plan state
 struct Stage {
     KParams kp;
+    const void* fn = nullptr;    // kernel entry (generic or statically shaped)
     unsigned grid;
     int threads;
     size_t smem;
     int cluster;
     int in_sel, out_sel;     // 0 user in, 1 user out, 2 scratch0, 3 scratch1
+    int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
 };
 
 struct Shape {
@@ -251,6 +265,26 @@ static bool rows_shape(int64_t M, int64_t nx, int conv, int dtype, int64_t batch
     return sh.smem <= kSmemMax;
 }
 
+// shared memory of a FOUR CTA: sub-transform twiddles, the two-level four-step
+// twiddle table, the data buffer, the Rader x chunk and the FP64 reduction
+// scratch (layout documented at four_body in engine.cuh)
+static int twolevel_bits(int64_t N) {
+    int bits = 0;
+    while ((1LL << (2 * bits)) < N) bits++;
+    return bits;
+}
+static size_t four_smem_bytes(int64_t M, int64_t N1, int64_t N2, int64_t bufsz, int64_t XP, size_t e) {
+    const int bits = twolevel_bits(M);
+    const int64_t nlo = 1LL << bits, nhi = (M + nlo - 1) / nlo + 1;
+    size_t b = (size_t)(N1 + N2) * e;
+    b = (b + 15) & ~(size_t)15;
+    b += (size_t)(nlo + nhi) * sizeof(double2);
+    b += (size_t)(bufsz + XP) * e;
+    b = (b + 15) & ~(size_t)15;
+    b += 48 * sizeof(double2);
+    return b;
+}
+
 static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vector<Shape>& out) {
     size_t e = elem_bytes(dtype);
     for (int64_t N1 = 2; N1 <= 4096; N1++) {
@@ -267,14 +301,13 @@ static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vec
             if (C == 1) {
                 PA = PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
             } else {
-                if (M / C > (int64_t)CFFT_THREADS * CFFT_EMAX) continue;
                 if (W < 2 || R1 < 2) continue;
                 PA = W;
                 PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
             }
             int64_t XP = (conv == CONV_RADER) ? (nx + C - 1) / C : 0;
-            int64_t bufsz = std::max(N1 * PA, R1 * PC);
-            size_t smem = (size_t)(bufsz + XP) * e + (32 + 16) * sizeof(double2) + 16;
+            int64_t bufsz = (C == 1) ? N1 * PA : N1 * PA + R1 * PC;
+            size_t smem = four_smem_bytes(M, N1, N2, bufsz, XP, e);
             if (smem > kSmemMax) continue;
             Shape sh;
             sh.mode = MODE_FOUR;
@@ -289,6 +322,12 @@ static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vec
             double bal = std::fabs(std::log2((double)N1 / (double)N2));
             sh.score = (smem > kSmemTwoPerSM ? 8.0 : 0.0) + (C > 8 ? 3.0 : 0.0) + 0.6 * C +
                        0.5 * bal + 0.1 * (ra.size() + rc.size());
+            // a statically shaped kernel for exactly this shape folds strides
+            // and counts to constants: prefer it
+            unsigned char ca[8], cc[8];
+            radix_counts(ra, ca);
+            radix_counts(rc, cc);
+            if (cfft_static_four(dtype, (int)N1, (int)N2, C, ca, cc)) sh.score -= 6.0;
             out.push_back(sh);
         }
     }
@@ -372,13 +411,28 @@ static int dev_upload(cfft_plan_s* P, const void* h, size_t bytes, void** d) {
     CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
     return CFFT_OK;
 }
-static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, SubPlan& sp) {
+static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, int64_t count,
+                        SubPlan& sp) {
     memset(&sp, 0, sizeof sp);
     sp.L = (int)L;
     sp.np = (int)rad.size();
     if (sp.np > CFFT_MAXP) return fail(CFFT_ERR_UNSUPPORTED, "too many radix passes");
-    for (int i = 0; i < sp.np; i++) sp.radix[i] = (unsigned char)rad[i];
+    // the device runs passes in canonical order 16, 9, 8, 7, 5, 4, 3, 2
+    int k = 0;
+    for (int ci = 0; ci < 8; ci++) {
+        int c = 0;
+        for (int r : rad) c += (r == kRadices[ci]);
+        sp.cnt[ci] = (unsigned char)c;
+        for (int j = 0; j < c; j++) sp.radix[k++] = (unsigned char)kRadices[ci];
+    }
+    if (k != sp.np) return fail(CFFT_ERR_UNSUPPORTED, "radix outside the codelet set");
     sp.G = std::max(1, wave_G(rad, L, CFFT_THREADS));
+    // warp-synchronous mode when a warp can own whole sub-transforms and
+    // there are enough of them to occupy every warp of the block
+    int gw = wave_G(rad, L, 32);
+    if (gw > 1 << 16) gw = 1 << 16;
+    sp.Gwarp = 0;
+    if (gw >= 1 && count >= (int64_t)(CFFT_THREADS / 32) * gw / 2) sp.Gwarp = gw;
     if (L <= 1) { sp.tw = nullptr; return CFFT_OK; }
     void* d = nullptr;
     int rc;
@@ -398,8 +452,7 @@ static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, 
     return rc;
 }
 static int make_twolevel(cfft_plan_s* P, int64_t N, TwoLevel& t) {
-    int bits = 0;
-    while ((1LL << (2 * bits)) < N) bits++;
+    const int bits = twolevel_bits(N);
     int64_t lo_n = 1LL << bits, hi_n = (N + lo_n - 1) / lo_n + 1;
     std::vector<double2> lo(lo_n), hi(hi_n);
     for (int64_t a = 0; a < lo_n; a++) lo[a] = omega(a, N, -1);
@@ -529,7 +582,10 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         kp.V = sh.V;
         kp.PC = (int)(sh.M + ((sh.M % 2 == 0) ? 1 : 0));
         kp.XP = (sh.conv == CONV_RADER) ? (int)P->n : 0;
-        rc = make_subplan(P, sh.M, sh.rc, kp.pc);
+        kp.mX = magic(P->n);
+        kp.mM = magic(sh.M);
+        kp.mL = magic(std::max<int64_t>(1, P->n - 1));
+        rc = make_subplan(P, sh.M, sh.rc, sh.V, kp.pc);
         if (rc) return rc;
         Stage s;
         s.kp = kp;
@@ -539,7 +595,8 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.grid = 0;  // set per execution from batch
         s.in_sel = 0;
         s.out_sel = 1;
-        CUDA_TRY(cfft_prepare_kernel(MODE_ROWS, P->dtype, s.smem, 1));
+        s.fn = cfft_kernel_for(MODE_ROWS, P->dtype);
+        CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, 1));
         P->stages.push_back(s);
         P->chunk = P->batch;
         return CFFT_OK;
@@ -556,9 +613,13 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
             kp.PC = sh.N2 + ((sh.N2 % 2 == 0) ? 1 : 0);
         }
         kp.XP = (sh.conv == CONV_RADER) ? (int)((P->n + sh.C - 1) / sh.C) : 0;
-        rc = make_subplan(P, sh.N1, sh.ra, kp.pa);
+        kp.mW = magic(sh.N2 / sh.C);
+        kp.mN2 = magic(sh.N2);
+        kp.mR1 = magic(sh.N1 / sh.C);
+        kp.mX = magic(std::max(kp.XP, 1));
+        rc = make_subplan(P, sh.N1, sh.ra, sh.N2 / sh.C, kp.pa);
         if (rc) return rc;
-        rc = make_subplan(P, sh.N2, sh.rc, kp.pc);
+        rc = make_subplan(P, sh.N2, sh.rc, sh.N1 / sh.C, kp.pc);
         if (rc) return rc;
         rc = make_twolevel(P, sh.M, kp.t4);
         if (rc) return rc;
@@ -570,16 +631,19 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.grid = 0;
         s.in_sel = 0;
         s.out_sel = 1;
-        CUDA_TRY(cfft_prepare_kernel(MODE_FOUR, P->dtype, s.smem, sh.C));
-        if (sh.C > 1) {
+        s.fn = cfft_static_four(P->dtype, sh.N1, sh.N2, sh.C, kp.pa.cnt, kp.pc.cnt);
+        if (s.fn) P->desc += "+static";
+        else s.fn = cfft_kernel_for(MODE_FOUR, P->dtype);
+        CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, sh.C));
+        {
             int nclusters = 0;
-            cudaError_t ce = cfft_max_active_clusters(MODE_FOUR, P->dtype, CFFT_THREADS, s.smem, sh.C,
-                                                      &nclusters);
+            cudaError_t ce = cfft_max_active_clusters_fn(s.fn, CFFT_THREADS, s.smem, sh.C, &nclusters);
             if (ce != cudaSuccess || nclusters < 1) {
                 cudaGetLastError();
                 return fail(CFFT_ERR_UNSUPPORTED, "cluster configuration not schedulable: C=" +
                                                       std::to_string(sh.C));
             }
+            s.max_units = nclusters;
         }
         P->stages.push_back(s);
         P->chunk = P->batch;
@@ -587,23 +651,22 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     }
     // two HBM passes per FFT_M (and two FFT_M for a convolution)
     const int64_t N1 = sh.N1, N2 = sh.N2, M = sh.M;
-    SubPlan pa, pc;
-    rc = make_subplan(P, N1, sh.ra, pa);
-    if (rc) return rc;
-    rc = make_subplan(P, N2, sh.rc, pc);
-    if (rc) return rc;
-    TwoLevel t4;
-    rc = make_twolevel(P, M, t4);
-    if (rc) return rc;
-    // tile widths: largest divisor with <= 96 KB of smem
+    const int64_t PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
     auto pick_tile = [&](int64_t count, int64_t per) {
         int64_t best = 1;
         for (int64_t v = 1; v <= count; v++)
             if (count % v == 0 && (size_t)(v * per) * e <= 96 * 1024 && v <= 64) best = v;
         return best;
     };
-    const int64_t PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
     const int64_t Vc = pick_tile(N2, N1), Vr = pick_tile(N1, PC);
+    SubPlan pa, pc;
+    rc = make_subplan(P, N1, sh.ra, Vc, pa);
+    if (rc) return rc;
+    rc = make_subplan(P, N2, sh.rc, Vr, pc);
+    if (rc) return rc;
+    TwoLevel t4;
+    rc = make_twolevel(P, M, t4);
+    if (rc) return rc;
     // chunk the batch so the scratch of one chunk stays within ~64 MB (L2 sized)
     const int nscr = (sh.conv == CONV_NONE) ? 1 : 2;
     int64_t chunk = std::max<int64_t>(1, (int64_t)(64LL << 20) / (int64_t)(M * e * nscr));
@@ -622,6 +685,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp.N2 = (int)N2;
         s.kp.V = (int)Vc;
         s.kp.PA = (int)Vc;
+        s.kp.mV = magic(Vc);
         s.kp.pa = pa;
         s.kp.t4 = t4;
         s.kp.pre = pre;
@@ -640,6 +704,8 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp.N2 = (int)N2;
         s.kp.V = (int)Vr;
         s.kp.PC = (int)PC;
+        s.kp.mV = magic(Vr);
+        s.kp.mN2 = magic(N2);
         s.kp.pc = pc;
         s.kp.post = post;
         s.threads = CFFT_THREADS;
@@ -658,7 +724,10 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         P->stages.push_back(col(PRE_SPEC, 3, 2));
         P->stages.push_back(row(POST_CHIRP, 2, 1));
     }
-    for (auto& s : P->stages) CUDA_TRY(cfft_prepare_kernel(s.kp.mode, P->dtype, s.smem, 1));
+    for (auto& s : P->stages) {
+        s.fn = cfft_kernel_for(s.kp.mode, P->dtype);
+        CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, 1));
+    }
     return CFFT_OK;
 }
 
@@ -686,6 +755,8 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
     const size_t e = elem_bytes(P->dtype);
     const int64_t n = P->n;
     const int64_t total = (nbatch < 0) ? P->batch : std::min(nbatch, P->batch);
+    if (((uintptr_t)in % e) != 0 || ((uintptr_t)out % e) != 0)
+        return fail(CFFT_ERR_INVALID, "buffers must be aligned to the element size");
     for (int64_t b0 = 0; b0 < total; b0 += P->chunk) {
         const int64_t nb = std::min(P->chunk, total - b0);
         for (auto& s : P->stages) {
@@ -707,7 +778,7 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             else if (kp.mode == MODE_FOUR) grid = (unsigned)(nb * kp.C);
             else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
             else grid = (unsigned)(nb * (kp.N1 / kp.V));
-            cudaError_t ce = cfft_launch(kp, P->dtype, grid, s.threads, s.smem, s.cluster, st);
+            cudaError_t ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             if (ce != cudaSuccess)
                 return fail(CFFT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
         }
