@@ -31,6 +31,7 @@ SIGNATURES = {
     "cfft_plan_workspace_bytes": (_i64, [_vp]),
     "cfft_plan_launches": (_ci, [_vp]),
     "cfft_version": (_ci, []),
+    "cfft_fft_twopass_noalloc": (_ci, [_i64, _i64, _ci, _vp, _vp, _ci, _vp]),
 }
 
 

@@ -20,3 +20,5 @@ cudaError_t cfft_prepare_fn(const void* fn, size_t smem, int cluster);
 cudaError_t cfft_launch_fn(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
                            int cluster, cudaStream_t stream);
 cudaError_t cfft_max_active_clusters_fn(const void* fn, int threads, size_t smem, int cluster, int* out);
+// set the thread-local text returned by cfft_last_error() (fixed buffer)
+void cfft_set_last_error(const char* msg);

@@ -26,9 +26,11 @@
 #include "../../include/catabra_b200.h"
 #include "kernels.h"
 
-static thread_local std::string g_err;
+// thread-local error text in a fixed buffer (set without touching the heap)
+static thread_local char g_err[512];
+void cfft_set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg ? msg : ""); }
 static int fail(int code, const std::string& msg) {
-    g_err = msg;
+    cfft_set_last_error(msg.c_str());
     return code;
 }
 #define CUDA_TRY(call)                                                                     \
@@ -855,7 +857,7 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
         std::string keep = g_err;
         plan_free(P);
         delete P;
-        g_err = keep;
+        cfft_set_last_error(keep.c_str());
         return rc;
     }
     *out = P;
@@ -870,10 +872,10 @@ extern "C" {
 
 int cfft_version(void) { return 100; }
 
-const char* cfft_last_error(void) { return g_err.c_str(); }
+const char* cfft_last_error(void) { return g_err; }
 
 int cfft_plan_create(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags) {
-    g_err.clear();
+    g_err[0] = 0;
     return plan_create_impl(plan, n, batch, dtype, flags);
 }
 

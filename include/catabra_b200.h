@@ -96,6 +96,18 @@ int64_t cfft_plan_workspace_bytes(cfft_plan plan);
 /* Number of kernel launches one cfft_execute of this plan issues. */
 int cfft_plan_launches(cfft_plan plan);
 
+/* No counterpart in the reference.  The two-pass FFT for callers that cannot
+ * allocate device memory (an allocator-owned or capture-time context): the
+ * scratch and twiddle tables live in one fixed __device__ array (32 MiB +
+ * 256 KiB per GPU, held until exit), so nothing is allocated.  n must be
+ * 7-smooth, split as N1*N2 with N1, N2 <= 4096, and hold at most 2^21
+ * ComplexF64 / 2^22 ComplexF32 elements; otherwise CFFT_ERR_UNSUPPORTED.
+ * The first call on a device does a one-time set-up (make it before any
+ * stream capture).  All calls share the array: calls that overlap on the
+ * GPU race -- serialise them. */
+int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, const void* d_in, void* d_out,
+                             int direction, void* stream);
+
 /* ABI version (major*100 + minor). */
 int cfft_version(void);
 
