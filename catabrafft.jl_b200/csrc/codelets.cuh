@@ -12,7 +12,7 @@ template <> __device__ __forceinline__ float2 mk<float2>(float x, float y) { ret
 
 // DFT_2, forward (w = exp(-2*pi*i/2)), in place on a[0..1]
 template <typename V>
-__device__ __forceinline__ void dft2(V* a) {
+__device__ __forceinline__ void dft2(V (&a)[2]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -24,7 +24,7 @@ __device__ __forceinline__ void dft2(V* a) {
 
 // DFT_3, forward (w = exp(-2*pi*i/3)), in place on a[0..2]
 template <typename V>
-__device__ __forceinline__ void dft3(V* a) {
+__device__ __forceinline__ void dft3(V (&a)[3]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -43,7 +43,7 @@ __device__ __forceinline__ void dft3(V* a) {
 
 // DFT_4, forward (w = exp(-2*pi*i/4)), in place on a[0..3]
 template <typename V>
-__device__ __forceinline__ void dft4(V* a) {
+__device__ __forceinline__ void dft4(V (&a)[4]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -66,7 +66,7 @@ __device__ __forceinline__ void dft4(V* a) {
 
 // DFT_5, forward (w = exp(-2*pi*i/5)), in place on a[0..4]
 template <typename V>
-__device__ __forceinline__ void dft5(V* a) {
+__device__ __forceinline__ void dft5(V (&a)[5]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -96,7 +96,7 @@ __device__ __forceinline__ void dft5(V* a) {
 
 // DFT_7, forward (w = exp(-2*pi*i/7)), in place on a[0..6]
 template <typename V>
-__device__ __forceinline__ void dft7(V* a) {
+__device__ __forceinline__ void dft7(V (&a)[7]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -137,7 +137,7 @@ __device__ __forceinline__ void dft7(V* a) {
 
 // DFT_8, forward (w = exp(-2*pi*i/8)), in place on a[0..7]
 template <typename V>
-__device__ __forceinline__ void dft8(V* a) {
+__device__ __forceinline__ void dft8(V (&a)[8]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -188,7 +188,7 @@ __device__ __forceinline__ void dft8(V* a) {
 
 // DFT_9, forward (w = exp(-2*pi*i/9)), in place on a[0..8]
 template <typename V>
-__device__ __forceinline__ void dft9(V* a) {
+__device__ __forceinline__ void dft9(V (&a)[9]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -258,7 +258,7 @@ __device__ __forceinline__ void dft9(V* a) {
 
 // DFT_16, forward (w = exp(-2*pi*i/16)), in place on a[0..15]
 template <typename V>
-__device__ __forceinline__ void dft16(V* a) {
+__device__ __forceinline__ void dft16(V (&a)[16]) {
     typedef typename real_of<V>::R R;
     const V a0 = a[0];
     const V a1 = a[1];
@@ -375,7 +375,7 @@ __device__ __forceinline__ void dft16(V* a) {
     a[15] = t81;
 }
 
-template <int RADIX, typename V> __device__ __forceinline__ void dft(V* a) {
+template <int RADIX, typename V> __device__ __forceinline__ void dft(V (&a)[RADIX]) {
     if constexpr (RADIX == 2) dft2(a);
     else if constexpr (RADIX == 3) dft3(a);
     else if constexpr (RADIX == 4) dft4(a);

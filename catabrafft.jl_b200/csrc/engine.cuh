@@ -131,11 +131,12 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // enumerated with carries instead of divisions.
 template <typename V, int EMAX, int R, bool WARP>
 __device__ __forceinline__ void spass(V* __restrict__ buf, int L, int Gw, int is, int gs, int s,
-                                      const V* __restrict__ tw) {
+                                      const V* __restrict__ twp) {
     constexpr int SL = EMAX / R;
     const int T = WARP ? 32 : (int)blockDim.x;
     const int tid = WARP ? (opaque_tid() & 31) : opaque_tid();
     const int nb = L / R;
+    const int n1 = nb / s;            // butterflies per stride class = twiddle block width
     const int W = Gw * nb;
     V v[SL][R];
     int off[SL], pp_[SL];
@@ -170,7 +171,7 @@ __device__ __forceinline__ void spass(V* __restrict__ buf, int L, int Gw, int is
             const int p0 = pp_[i];
             if (p0) {
 #pragma unroll
-                for (int j = 1; j < R; j++) v[i][j] = cmul(v[i][j], tw[j * p0 * s]);
+                for (int j = 1; j < R; j++) v[i][j] = cmul(v[i][j], twp[(j - 1) * n1 + p0]);
             }
             V* dst = buf + off[i];
 #pragma unroll
@@ -180,9 +181,9 @@ __device__ __forceinline__ void spass(V* __restrict__ buf, int L, int Gw, int is
     if (WARP) __syncwarp(); else __syncthreads();
 }
 
-// All passes of `count` sub-transforms, pass-major.  The radix sequence is
-// canonical -- 16^a 9^b 8^c 7^d 5^e 4^f 3^g 2^h, multiplicities in P.cnt[] --
-// and runs as eight fixed-radix loops with runtime trip counts: every pass
+// All passes of `count` sub-transforms, pass-major.  The radix sequence runs
+// in CFFT_EXEC_ORDER -- 9^a 7^b 5^c 3^d 16^e 8^f 4^g 2^h, multiplicities in
+// P.cnt[] -- as eight fixed-radix loops with runtime trip counts: every pass
 // body is a compile-time radix, so no runtime switch widens the register live
 // ranges (a switch over radices spills FP64 codelets).
 // Block mode: waves of P.G whole sub-transforms (disjoint element sets, so
@@ -191,42 +192,51 @@ __device__ __forceinline__ void spass(V* __restrict__ buf, int L, int Gw, int is
 // (w, w + nwarps, ...) and never waits for the other warps.
 // Caller must have synchronised the block after writing buf; returns
 // synchronised.
-template <typename V, int EMAX, int R>
+// WM selects the team at compile time (0 block, 1 warp) or at run time from
+// P.Gwarp (2).  Kernels that must serve both instantiate 0 and 1 separately:
+// with both variants in one FP32 function the compiler demotes the register
+// arrays to local memory.
+template <typename V, int EMAX, int R, int WM>
 __device__ __forceinline__ void radix_loop(V* buf, const SubPlan& P, int count, int is, int gs, int& s,
-                                           const V* tw, int cnt) {
-    if (P.Gwarp > 0) {
+                                           const V*& twp, int cnt) {
+    const bool warp = (WM == 1) || (WM == 2 && P.Gwarp > 0);
+    if (WM != 0 && warp) {
         const int nw = blockDim.x >> 5, wid = opaque_tid() >> 5;
         const int step = nw * P.Gwarp;
         for (int i = 0; i < cnt; i++) {
             for (int g0 = wid * P.Gwarp; g0 < count; g0 += step)
-                spass<V, EMAX, R, true>(buf + g0 * gs, P.L, min(P.Gwarp, count - g0), is, gs, s, tw);
+                spass<V, EMAX, R, true>(buf + g0 * gs, P.L, min(P.Gwarp, count - g0), is, gs, s, twp);
+            twp += (R - 1) * (P.L / (s * R));
             s *= R;
         }
-    } else {
+    } else if (WM != 1) {
         for (int i = 0; i < cnt; i++) {
             for (int g0 = 0; g0 < count; g0 += P.G)
-                spass<V, EMAX, R, false>(buf + g0 * gs, P.L, min(P.G, count - g0), is, gs, s, tw);
+                spass<V, EMAX, R, false>(buf + g0 * gs, P.L, min(P.G, count - g0), is, gs, s, twp);
+            twp += (R - 1) * (P.L / (s * R));
             s *= R;
         }
     }
 }
-template <typename V, int EMAX>
+template <typename V, int EMAX, int WM = 2>
 __device__ __forceinline__ void run_subffts(V* buf, const SubPlan& P, const V* tw, int count, int is,
                                             int gs) {
     int s = 1;
-    radix_loop<V, EMAX, 16>(buf, P, count, is, gs, s, tw, P.cnt[0]);
-    radix_loop<V, EMAX, 9>(buf, P, count, is, gs, s, tw, P.cnt[1]);
-    radix_loop<V, EMAX, 8>(buf, P, count, is, gs, s, tw, P.cnt[2]);
-    radix_loop<V, EMAX, 7>(buf, P, count, is, gs, s, tw, P.cnt[3]);
-    radix_loop<V, EMAX, 5>(buf, P, count, is, gs, s, tw, P.cnt[4]);
-    radix_loop<V, EMAX, 4>(buf, P, count, is, gs, s, tw, P.cnt[5]);
-    radix_loop<V, EMAX, 3>(buf, P, count, is, gs, s, tw, P.cnt[6]);
-    radix_loop<V, EMAX, 2>(buf, P, count, is, gs, s, tw, P.cnt[7]);
-    if (P.Gwarp > 0) __syncthreads();
+    const V* twp = tw;
+    // CFFT_EXEC_ORDER
+    radix_loop<V, EMAX, 9, WM>(buf, P, count, is, gs, s, twp, P.cnt[0]);
+    radix_loop<V, EMAX, 7, WM>(buf, P, count, is, gs, s, twp, P.cnt[1]);
+    radix_loop<V, EMAX, 5, WM>(buf, P, count, is, gs, s, twp, P.cnt[2]);
+    radix_loop<V, EMAX, 3, WM>(buf, P, count, is, gs, s, twp, P.cnt[3]);
+    radix_loop<V, EMAX, 16, WM>(buf, P, count, is, gs, s, twp, P.cnt[4]);
+    radix_loop<V, EMAX, 8, WM>(buf, P, count, is, gs, s, twp, P.cnt[5]);
+    radix_loop<V, EMAX, 4, WM>(buf, P, count, is, gs, s, twp, P.cnt[6]);
+    radix_loop<V, EMAX, 2, WM>(buf, P, count, is, gs, s, twp, P.cnt[7]);
+    if (WM == 1 || (WM == 2 && P.Gwarp > 0)) __syncthreads();
 }
 template <typename V, int EMAX>
 __device__ __forceinline__ void run_subffts(V* buf, const SubPlan& P, int count, int is, int gs) {
-    run_subffts<V, EMAX>(buf, P, (const V*)P.tw, count, is, gs);
+    run_subffts<V, EMAX, 2>(buf, P, (const V*)P.tw, count, is, gs);
 }
 
 // block-wide FP64 complex sum (result valid in every thread)
@@ -354,10 +364,12 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
 // Column layout (step A): (i1, j) at i1*PA + j, j < W = N2/C
 // Row layout    (step C): (r, i2) at r*PC + i2, r < N1/C
 //
-// The body is written once against a shape policy K: DynK reads the shape
-// from KParams (any size the planner picks), StatK<...> fixes it at compile
-// time for the hot sizes so strides, counts and divisions fold to constants.
-struct DynK {
+// The body is written once against a shape policy K: DynK<WM> reads the shape
+// from KParams (any size the planner picks; WM = 1 when both sub-plans run
+// warp-synchronous, 0 when both run block-wide), StatK<...> fixes it at
+// compile time for the hot sizes so strides, counts and divisions fold to
+// constants.
+template <int WM> struct DynK {
     __device__ static int N1(const KParams& p) { return p.N1; }
     __device__ static int N2(const KParams& p) { return p.N2; }
     __device__ static int C(const KParams& p) { return p.C; }
@@ -368,19 +380,20 @@ struct DynK {
     __device__ static int dW(const KParams& p, unsigned x) { return fdiv(x, p.mW); }
     __device__ static int dN2(const KParams& p, unsigned x) { return fdiv(x, p.mN2); }
     __device__ static int dR1(const KParams& p, unsigned x) { return fdiv(x, p.mR1); }
-    template <typename V, int EMAX> __device__ static void colA(V* buf, const KParams& p, const V* tw) {
-        run_subffts<V, EMAX>(buf, p.pa, tw, p.N2 / p.C, p.PA, 1);
+    template <typename V, int EMAX> __device__ __forceinline__ static void colA(V* buf, const KParams& p, const V* tw) {
+        run_subffts<V, EMAX, WM>(buf, p.pa, tw, p.N2 / p.C, p.PA, 1);
     }
-    template <typename V, int EMAX> __device__ static void rowC(V* buf, const KParams& p, const V* tw) {
-        run_subffts<V, EMAX>(buf, p.pc, tw, p.N1 / p.C, 1, p.PC);
+    template <typename V, int EMAX> __device__ __forceinline__ static void rowC(V* buf, const KParams& p, const V* tw) {
+        run_subffts<V, EMAX, WM>(buf, p.pc, tw, p.N1 / p.C, 1, p.PC);
     }
 };
 
 // compile-time radix sequence (canonical order) and its pass chain
 template <int... R> struct Seq {};
-template <typename V, int EMAX, bool WARP, int L, int IS, int GS, int COUNT, int GW, int S, int R,
-          int... Rest>
-__device__ __forceinline__ void st_passes(V* buf, const V* tw) {
+template <typename V, int EMAX, bool WARP, int L, int IS, int GS, int COUNT, int GW, int S, int OFF,
+          int R, int... Rest>
+__device__ __forceinline__ void st_passes(V* buf, const V* tw0) {
+    const V* tw = tw0 + OFF;
     if constexpr (WARP) {
         const int nw = blockDim.x >> 5, wid = opaque_tid() >> 5;
         for (int g0 = wid * GW; g0 < COUNT; g0 += nw * GW) {
@@ -395,11 +408,12 @@ __device__ __forceinline__ void st_passes(V* buf, const V* tw) {
             spass<V, EMAX, R, false>(buf + g0 * GS, L, (COUNT - g0 < GW) ? COUNT - g0 : GW, IS, GS, S, tw);
     }
     if constexpr (sizeof...(Rest) > 0)
-        st_passes<V, EMAX, WARP, L, IS, GS, COUNT, GW, S * R, Rest...>(buf, tw);
+        st_passes<V, EMAX, WARP, L, IS, GS, COUNT, GW, S * R, OFF + (R - 1) * (L / (S * R)), Rest...>(buf,
+                                                                                                     tw0);
 }
 template <typename V, int EMAX, bool WARP, int L, int IS, int GS, int COUNT, int GW, int... R>
 __device__ __forceinline__ void st_subffts(V* buf, const V* tw, Seq<R...>) {
-    st_passes<V, EMAX, WARP, L, IS, GS, COUNT, GW, 1, R...>(buf, tw);
+    st_passes<V, EMAX, WARP, L, IS, GS, COUNT, GW, 1, 0, R...>(buf, tw);
     if constexpr (WARP) __syncthreads();
 }
 
@@ -418,10 +432,10 @@ struct StatK {
     __device__ static int dW(const KParams&, unsigned x) { return (int)(x / (unsigned)kW); }
     __device__ static int dN2(const KParams&, unsigned x) { return (int)(x / (unsigned)N2_); }
     __device__ static int dR1(const KParams&, unsigned x) { return (int)(x / (unsigned)kR1); }
-    template <typename V, int EMAX> __device__ static void colA(V* buf, const KParams&, const V* tw) {
+    template <typename V, int EMAX> __device__ __forceinline__ static void colA(V* buf, const KParams&, const V* tw) {
         st_subffts<V, EMAX, WA, N1_, kPA, 1, kW, GA>(buf, tw, SA{});
     }
-    template <typename V, int EMAX> __device__ static void rowC(V* buf, const KParams&, const V* tw) {
+    template <typename V, int EMAX> __device__ __forceinline__ static void rowC(V* buf, const KParams&, const V* tw) {
         st_subffts<V, EMAX, WC, N2_, 1, kPC, kR1, GC>(buf, tw, SC{});
     }
 };
@@ -478,7 +492,7 @@ __device__ __forceinline__ void four_twiddle_local(const KParams& p, V* buf, con
 }
 
 // Shared-memory carve-up of a FOUR CTA (host and device agree on it):
-//   twA[N1] twC[N2] (V)  t4lo[2^bits] t4hi[nhi] (FP64)  bufA[N1*PA]
+//   twA[pa.twlen] twC[pc.twlen] (V)  t4lo[2^bits] t4hi[nhi] (FP64)  bufA[N1*PA]
 //   bufC[R1*PC] (C > 1 only; C = 1 works in place)  xs[XP] (Rader)
 //   red[48] (FP64, 16-byte aligned)
 // One transform per cluster.  The CTA first issues cp.async copies of its
@@ -668,9 +682,10 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
     const int N1 = K::N1(p), N2 = K::N2(p);
     const int nlo = 1 << p.t4.bits, nhi = (p.t4.N + nlo - 1) / nlo + 1;
 
+    const int lA = p.pa.twlen, lC = p.pc.twlen;
     V* twA = (V*)smem;
-    V* twC = twA + N1;
-    double2* t4lo = after16(twC + N2);
+    V* twC = twA + lA;
+    double2* t4lo = after16(twC + lC);
     double2* t4hi = t4lo + nlo;
     V* buf = (V*)(t4hi + nhi);            // column layout (N1 x PA)
     V* bufC = (C > 1) ? buf + N1 * K::PA(p) : buf;   // row layout (R1 x PC)
@@ -679,8 +694,8 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
 
     four_prefetch<V, K>(p, buf, t, c);
     // tables -> shared memory while the input is in flight
-    for (int i = tid; i < N1; i += T) twA[i] = ((const V*)p.pa.tw)[i];
-    for (int i = tid; i < N2; i += T) twC[i] = ((const V*)p.pc.tw)[i];
+    for (int i = tid; i < lA; i += T) twA[i] = ((const V*)p.pa.tw)[i];
+    for (int i = tid; i < lC; i += T) twC[i] = ((const V*)p.pc.tw)[i];
     for (int i = tid; i < nlo; i += T) t4lo[i] = p.t4.lo[i];
     for (int i = tid; i < nhi; i += T) t4hi[i] = p.t4.hi[i];
     TwoLevel t4 = p.t4;

@@ -4,14 +4,23 @@
 
 #define CFFT_MAXP 24
 
+// Radix passes run in this order: odd radices first, so that the first
+// pass's stride-R writes never hit a multiple of 8 elements (which would
+// put a quarter-warp of 16-byte stores on one bank group).
+#define CFFT_EXEC_ORDER {9, 7, 5, 3, 16, 8, 4, 2}
+
 struct SubPlan {
     int L;                        // sub-transform length
     int np;                       // number of radix passes
     int G;                        // sub-transforms per block-wide wave (fits EMAX regs/thread)
     int Gwarp;                    // sub-transforms per warp group (0: block mode)
-    unsigned char radix[CFFT_MAXP];  // pass radices in execution order (canonical)
-    unsigned char cnt[8];         // multiplicities of 16, 9, 8, 7, 5, 4, 3, 2
-    const void* tw;               // w_L^m, m < L, element type of the data
+    unsigned char radix[CFFT_MAXP];  // pass radices in execution order
+    unsigned char cnt[8];         // multiplicities of 9, 7, 5, 3, 16, 8, 4, 2 (CFFT_EXEC_ORDER)
+    int twlen;                    // entries of tw
+    // per-pass twiddle blocks in execution order: pass p (stride s, n1 =
+    // L/(s r)) owns (r-1)*n1 entries, tw[off + (j-1)*n1 + q] = w_L^(j*q*s),
+    // so adjacent lanes (adjacent q) read adjacent entries
+    const void* tw;
 };
 
 struct TwoLevel {                 // w_N^e = lo[e & mask] * hi[e >> bits]  (FP64)
@@ -22,6 +31,9 @@ struct TwoLevel {                 // w_N^e = lo[e & mask] * hi[e >> bits]  (FP64
 };
 
 enum { MODE_ROWS = 0, MODE_FOUR = 1, MODE_COLPASS = 2, MODE_ROWPASS = 3 };
+// kernel selector only (KParams.mode stays MODE_FOUR): the generic four-step
+// kernel instantiated with warp-synchronous sub-transforms
+enum { MODE_FOUR_WARP = 16 };
 enum { CONV_NONE = 0, CONV_RADER = 1, CONV_BLUE = 2 };
 enum { PRE_NONE = 0, PRE_CHIRP = 1, PRE_SPEC = 2 };      // COLPASS prologue
 enum { POST_OUT = 0, POST_RAW = 1, POST_CHIRP = 2 };     // ROWPASS epilogue

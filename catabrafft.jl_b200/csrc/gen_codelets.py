@@ -184,7 +184,7 @@ def gen(r: int) -> str:
     outs = e.dft(xs)
     head = [f"// DFT_{r}, forward (w = exp(-2*pi*i/{r})), in place on a[0..{r - 1}]",
             "template <typename V>",
-            f"__device__ __forceinline__ void dft{r}(V* a) {{",
+            f"__device__ __forceinline__ void dft{r}(V (&a)[{r}]) {{",
             "    typedef typename real_of<V>::R R;"]
     head += [f"    const V a{i} = a[{i}];" for i in range(r)]
     tail = [f"    a[{i}] = {o};" for i, o in enumerate(outs)]
@@ -211,7 +211,7 @@ def main():
     ]
     for r in RADICES:
         out.append(gen(r))
-    out.append("template <int RADIX, typename V> __device__ __forceinline__ void dft(V* a) {")
+    out.append("template <int RADIX, typename V> __device__ __forceinline__ void dft(V (&a)[RADIX]) {")
     for i, r in enumerate(RADICES):
         kw = "if constexpr" if i == 0 else "else if constexpr"
         out.append(f"    {kw} (RADIX == {r}) dft{r}(a);")

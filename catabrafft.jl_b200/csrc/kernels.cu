@@ -33,14 +33,16 @@ const void* cfft_kernel_for(int mode, int dtype) {
     if (dtype == CFFT_DT_C128) {
         switch (mode) {
             case MODE_ROWS: return (const void*)k_rows<double2, CFFT_EMAX>;
-            case MODE_FOUR: return (const void*)k_four<double2, CFFT_EMAX, DynK>;
+            case MODE_FOUR: return (const void*)k_four<double2, CFFT_EMAX, DynK<0>>;
+            case MODE_FOUR_WARP: return (const void*)k_four<double2, CFFT_EMAX, DynK<1>>;
             case MODE_COLPASS: return (const void*)k_colpass<double2, CFFT_EMAX>;
             case MODE_ROWPASS: return (const void*)k_rowpass<double2, CFFT_EMAX>;
         }
     } else {
         switch (mode) {
             case MODE_ROWS: return (const void*)k_rows<float2, CFFT_EMAX>;
-            case MODE_FOUR: return (const void*)k_four<float2, CFFT_EMAX, DynK>;
+            case MODE_FOUR: return (const void*)k_four<float2, CFFT_EMAX, DynK<0>>;
+            case MODE_FOUR_WARP: return (const void*)k_four<float2, CFFT_EMAX, DynK<1>>;
             case MODE_COLPASS: return (const void*)k_colpass<float2, CFFT_EMAX>;
             case MODE_ROWPASS: return (const void*)k_rowpass<float2, CFFT_EMAX>;
         }
@@ -49,29 +51,31 @@ const void* cfft_kernel_for(int mode, int dtype) {
 }
 
 // ---- statically shaped FOUR kernels for the hot lengths
-// radix multiplicities are listed in the canonical order 16, 9, 8, 7, 5, 4, 3, 2
+// radix multiplicities are listed in CFFT_EXEC_ORDER (9, 7, 5, 3, 16, 8, 4, 2)
+// and each Seq<> names the passes in that order
 struct StaticFour {
     int dtype, N1, N2, C;
     unsigned char ca[8], cc[8];
     const void* fn;
 };
 // 30240 = 168 x 180 on a 12-CTA cluster (ComplexF64 mixed-radix batch)
-using K_168x180_c12 = StatK<168, 180, 12, Seq<8, 7, 3>, true, 1, Seq<9, 5, 4>, true, 1>;
+using K_168x180_c12 = StatK<168, 180, 12, Seq<7, 3, 8>, true, 1, Seq<9, 5, 4>, true, 1>;
 // Rader M = 20160 = 168 x 120 on an 8-CTA cluster (primes 10007 .. 10081)
-using K_168x120_c8 = StatK<168, 120, 8, Seq<8, 7, 3>, true, 1, Seq<8, 5, 3>, true, 3>;
+using K_168x120_c8 = StatK<168, 120, 8, Seq<7, 3, 8>, true, 1, Seq<5, 3, 8>, true, 3>;
 // 65536 = 256 x 256 on a 16-CTA cluster (ComplexF32 precision form)
 using K_256x256_c16 = StatK<256, 256, 16, Seq<16, 16>, true, 2, Seq<16, 16>, true, 2>;
 
 static const StaticFour kStatic[] = {
-    {CFFT_DT_C128, 168, 180, 12, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 1, 0, 0, 1, 1, 0, 0},
+    //                        9  7  5  3 16  8  4  2
+    {CFFT_DT_C128, 168, 180, 12, {0, 1, 0, 1, 0, 1, 0, 0}, {1, 0, 1, 0, 0, 0, 1, 0},
      (const void*)k_four<double2, CFFT_EMAX, K_168x180_c12>},
-    {CFFT_DT_C64, 168, 180, 12, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 1, 0, 0, 1, 1, 0, 0},
+    {CFFT_DT_C64, 168, 180, 12, {0, 1, 0, 1, 0, 1, 0, 0}, {1, 0, 1, 0, 0, 0, 1, 0},
      (const void*)k_four<float2, CFFT_EMAX, K_168x180_c12>},
-    {CFFT_DT_C128, 168, 120, 8, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 0, 1, 0, 1, 0, 1, 0},
+    {CFFT_DT_C128, 168, 120, 8, {0, 1, 0, 1, 0, 1, 0, 0}, {0, 0, 1, 1, 0, 1, 0, 0},
      (const void*)k_four<double2, CFFT_EMAX, K_168x120_c8>},
-    {CFFT_DT_C64, 168, 120, 8, {0, 0, 1, 1, 0, 0, 1, 0}, {0, 0, 1, 0, 1, 0, 1, 0},
+    {CFFT_DT_C64, 168, 120, 8, {0, 1, 0, 1, 0, 1, 0, 0}, {0, 0, 1, 1, 0, 1, 0, 0},
      (const void*)k_four<float2, CFFT_EMAX, K_168x120_c8>},
-    {CFFT_DT_C64, 256, 256, 16, {2, 0, 0, 0, 0, 0, 0, 0}, {2, 0, 0, 0, 0, 0, 0, 0},
+    {CFFT_DT_C64, 256, 256, 16, {0, 0, 0, 0, 2, 0, 0, 0}, {0, 0, 0, 0, 2, 0, 0, 0},
      (const void*)k_four<float2, CFFT_EMAX, K_256x256_c16>},
 };
 
@@ -118,7 +122,9 @@ cudaError_t cfft_launch_fn(const void* f, const KParams& p, unsigned grid, int t
         cfg.numAttrs = 1;
     }
     void* args[] = {(void*)&p};
-    return cudaLaunchKernelExC(&cfg, f, args);
+    cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+    if (e != cudaSuccess) cudaGetLastError();   // do not leave it for the caller's next check
+    return e;
 }
 
 cudaError_t cfft_max_active_clusters_fn(const void* f, int threads, size_t smem, int cluster, int* out) {

@@ -73,33 +73,54 @@ __device__ double2 omega_dev(long long m, long long L) {
     sincospi(-2.0 * (double)m / (double)L, &s, &c);
     return make_double2(c, s);
 }
+// per-pass twiddle blocks of one sub-transform (layout of SubPlan.tw)
+struct PassTable {
+    int L, np, twlen;
+    int r[CFFT_MAXP], s[CFFT_MAXP], off[CFFT_MAXP];
+};
 template <typename V>
-__global__ void k_noalloc_tables(V* twA, int N1, V* twC, int N2, double2* lo, int nlo, double2* hi,
-                                 int nhi, int M) {
+__global__ void k_noalloc_tables(V* twA, PassTable A, V* twC, PassTable Cc, double2* lo, int nlo,
+                                 double2* hi, int nhi, int M) {
     const int stride = gridDim.x * blockDim.x;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 8192; i += stride) {
-        if (i < N1) { double2 w = omega_dev(i, N1); twA[i] = round_to<V>(w.x, w.y); }
-        if (i < N2) { double2 w = omega_dev(i, N2); twC[i] = round_to<V>(w.x, w.y); }
+    const int total = max(max(A.twlen, Cc.twlen), max(nlo, nhi));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        for (int w = 0; w < 2; w++) {
+            const PassTable& T = w ? Cc : A;
+            V* dst = w ? twC : twA;
+            if (i >= T.twlen) continue;
+            int p = 0;
+            while (p + 1 < T.np && T.off[p + 1] <= i) p++;
+            const int n1 = T.L / (T.s[p] * T.r[p]), k = i - T.off[p];
+            const int j = k / n1 + 1, q = k - (j - 1) * n1;
+            const double2 v = omega_dev((long long)j * q * T.s[p], T.L);
+            dst[i] = round_to<V>(v.x, v.y);
+        }
         if (i < nlo) lo[i] = omega_dev(i, M);
         if (i < nhi) hi[i] = omega_dev((long long)i * nlo, M);
     }
 }
 
-// canonical radix split (16, 9, 8, 7, 5, 4, 3, 2) into a fixed array
+// greedy radix split (largest codelet first), passes stored in CFFT_EXEC_ORDER
 const int kRad[8] = {16, 9, 8, 7, 5, 4, 3, 2};
+const int kExec[8] = CFFT_EXEC_ORDER;
 bool split_canonical(long long L, SubPlan& sp) {
     sp.L = (int)L;
     sp.np = 0;
     for (int i = 0; i < 8; i++) sp.cnt[i] = 0;
-    while (L > 1) {
+    long long rem = L;
+    while (rem > 1) {
         int k = -1;
         for (int i = 0; i < 8; i++)
-            if (L % kRad[i] == 0) { k = i; break; }
+            if (rem % kRad[i] == 0) { k = i; break; }
         if (k < 0 || sp.np >= CFFT_MAXP) return false;
-        sp.radix[sp.np++] = (unsigned char)kRad[k];
-        sp.cnt[k]++;
-        L /= kRad[k];
+        for (int i = 0; i < 8; i++)
+            if (kExec[i] == kRad[k]) sp.cnt[i]++;
+        sp.np++;
+        rem /= kRad[k];
     }
+    int k = 0;
+    for (int i = 0; i < 8; i++)
+        for (int c = 0; c < sp.cnt[i]; c++) sp.radix[k++] = (unsigned char)kExec[i];
     // block-wide waves only: G sub-transforms per wave fit 256 threads x 16 elements
     long long g = 1 << 20;
     for (int i = 0; i < sp.np; i++) {
@@ -109,6 +130,19 @@ bool split_canonical(long long L, SubPlan& sp) {
     sp.G = (int)std::max<long long>(1, std::min<long long>(g, 1 << 20));
     sp.Gwarp = 0;
     return sp.np == 0 || g >= 1;
+}
+void pass_table(const SubPlan& sp, PassTable& T) {
+    T.L = sp.L;
+    T.np = sp.np;
+    long long s = 1, off = 0;
+    for (int i = 0; i < sp.np; i++) {
+        T.r[i] = sp.radix[i];
+        T.s[i] = (int)s;
+        T.off[i] = (int)off;
+        off += (long long)(sp.radix[i] - 1) * (sp.L / (s * sp.radix[i]));
+        s *= sp.radix[i];
+    }
+    T.twlen = (int)off;
 }
 unsigned long long magic(long long d) {
     return ((1ULL << 40) + (unsigned long long)d - 1) / (unsigned long long)d;
@@ -169,8 +203,11 @@ extern "C" int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, con
             ce = cudaGetSymbolAddress(&ptr, g_noalloc_arena);
             if (ce != cudaSuccess || !ptr)
                 return noalloc_fail(CFFT_ERR_CUDA, "cudaGetSymbolAddress", ce);
-            ce = cfft_prepare_fn(fcol, 96 * 1024 + 16, 1);
-            if (ce == cudaSuccess) ce = cfft_prepare_fn(frow, 96 * 1024 + 16, 1);
+            // shared-memory attributes for both element types' pass kernels
+            for (int dt = 0; dt < 2 && ce == cudaSuccess; dt++) {
+                ce = cfft_prepare_fn(cfft_kernel_for(MODE_COLPASS, dt), 96 * 1024 + 16, 1);
+                if (ce == cudaSuccess) ce = cfft_prepare_fn(cfft_kernel_for(MODE_ROWPASS, dt), 96 * 1024 + 16, 1);
+            }
             if (ce != cudaSuccess) return noalloc_fail(CFFT_ERR_CUDA, "kernel attributes", ce);
             g_arena_ptr[dev] = (unsigned char*)ptr;
         }
@@ -183,19 +220,24 @@ extern "C" int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, con
     while ((1LL << (2 * bits)) < n) bits++;
     const int nlo = 1 << bits, nhi = (int)((n + nlo - 1) / nlo + 1);
     unsigned char* tab = arena + kScratchBytes;
+    PassTable TA, TC;
+    pass_table(pa, TA);
+    pass_table(pc, TC);
+    pa.twlen = TA.twlen;
+    pc.twlen = TC.twlen;
     void* twA = tab;
-    void* twC = tab + N1 * e;
-    size_t off = (size_t)((N1 + N2) * e + 255) & ~(size_t)255;
+    void* twC = tab + (size_t)TA.twlen * e;
+    size_t off = (size_t)((TA.twlen + TC.twlen) * e + 255) & ~(size_t)255;
     double2* lo = (double2*)(tab + off);
     double2* hi = lo + nlo;
     if (off + (size_t)(nlo + nhi) * sizeof(double2) > kTableBytes)
         return noalloc_fail(CFFT_ERR_UNSUPPORTED, "twiddle tables exceed the fixed table region");
     if (dtype == CFFT_C128)
-        k_noalloc_tables<double2><<<32, 256, 0, st>>>((double2*)twA, (int)N1, (double2*)twC, (int)N2, lo,
-                                                        nlo, hi, nhi, (int)n);
+        k_noalloc_tables<double2><<<32, 256, 0, st>>>((double2*)twA, TA, (double2*)twC, TC, lo, nlo, hi,
+                                                        nhi, (int)n);
     else
-        k_noalloc_tables<float2><<<32, 256, 0, st>>>((float2*)twA, (int)N1, (float2*)twC, (int)N2, lo,
-                                                       nlo, hi, nhi, (int)n);
+        k_noalloc_tables<float2><<<32, 256, 0, st>>>((float2*)twA, TA, (float2*)twC, TC, lo, nlo, hi,
+                                                       nhi, (int)n);
     ce = cudaGetLastError();
     if (ce != cudaSuccess) return noalloc_fail(CFFT_ERR_CUDA, "table kernel launch", ce);
 

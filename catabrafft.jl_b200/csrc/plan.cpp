@@ -90,7 +90,8 @@ static int64_t primitive_root(int64_t p) {
 
 // greedy radix split, largest first (create_std_radix_plan, radix_plan.jl:100-138,
 // over the codelet set of this build)
-static const int kRadices[] = {16, 9, 8, 7, 5, 4, 3, 2};
+static const int kRadices[] = {16, 9, 8, 7, 5, 4, 3, 2};   // split preference
+static const int kExec[] = CFFT_EXEC_ORDER;                  // execution order
 static std::vector<int> radix_split(int64_t L, const int* order = kRadices, int nord = 8) {
     std::vector<int> r;
     while (L > 1) {
@@ -111,9 +112,26 @@ static unsigned long long magic(int64_t d) {
 static void radix_counts(const std::vector<int>& rad, unsigned char* cnt) {
     for (int ci = 0; ci < 8; ci++) {
         int c = 0;
-        for (int r : rad) c += (r == kRadices[ci]);
+        for (int r : rad) c += (r == kExec[ci]);
         cnt[ci] = (unsigned char)c;
     }
+}
+// radices of a split in execution order
+static std::vector<int> exec_order(const std::vector<int>& rad) {
+    std::vector<int> out;
+    for (int ci = 0; ci < 8; ci++)
+        for (int r : rad)
+            if (r == kExec[ci]) out.push_back(r);
+    return out;
+}
+// entries of the per-pass twiddle table of a sub-transform
+static int64_t twiddle_len(int64_t L, const std::vector<int>& rad) {
+    int64_t s = 1, len = 0;
+    for (int r : exec_order(rad)) {
+        len += (int64_t)(r - 1) * (L / (s * r));
+        s *= r;
+    }
+    return len;
 }
 static int wave_G(const std::vector<int>& rad, int64_t L, int T) {
     if (L <= 1) return 1 << 20;
@@ -239,7 +257,9 @@ static size_t elem_bytes(int dtype) { return dtype == CFFT_C128 ? 16 : 8; }
 static const size_t kSmemMax = 220 * 1024;
 static const size_t kSmemTwoPerSM = 110 * 1024;
 
-static std::string join(const std::vector<int>& v) {
+static std::vector<int> exec_order(const std::vector<int>& rad);
+static std::string join(const std::vector<int>& v0) {
+    const std::vector<int> v = exec_order(v0);
     std::string s;
     for (size_t i = 0; i < v.size(); i++) s += (i ? "," : "") + std::to_string(v[i]);
     return s;
@@ -275,10 +295,10 @@ static int twolevel_bits(int64_t N) {
     while ((1LL << (2 * bits)) < N) bits++;
     return bits;
 }
-static size_t four_smem_bytes(int64_t M, int64_t N1, int64_t N2, int64_t bufsz, int64_t XP, size_t e) {
+static size_t four_smem_bytes(int64_t M, int64_t twA, int64_t twC, int64_t bufsz, int64_t XP, size_t e) {
     const int bits = twolevel_bits(M);
     const int64_t nlo = 1LL << bits, nhi = (M + nlo - 1) / nlo + 1;
-    size_t b = (size_t)(N1 + N2) * e;
+    size_t b = (size_t)(twA + twC) * e;
     b = (b + 15) & ~(size_t)15;
     b += (size_t)(nlo + nhi) * sizeof(double2);
     b += (size_t)(bufsz + XP) * e;
@@ -309,7 +329,7 @@ static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vec
             }
             int64_t XP = (conv == CONV_RADER) ? (nx + C - 1) / C : 0;
             int64_t bufsz = (C == 1) ? N1 * PA : N1 * PA + R1 * PC;
-            size_t smem = four_smem_bytes(M, N1, N2, bufsz, XP, e);
+            size_t smem = four_smem_bytes(M, twiddle_len(N1, ra), twiddle_len(N2, rc), bufsz, XP, e);
             if (smem > kSmemMax) continue;
             Shape sh;
             sh.mode = MODE_FOUR;
@@ -419,15 +439,13 @@ static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, 
     sp.L = (int)L;
     sp.np = (int)rad.size();
     if (sp.np > CFFT_MAXP) return fail(CFFT_ERR_UNSUPPORTED, "too many radix passes");
-    // the device runs passes in canonical order 16, 9, 8, 7, 5, 4, 3, 2
-    int k = 0;
-    for (int ci = 0; ci < 8; ci++) {
-        int c = 0;
-        for (int r : rad) c += (r == kRadices[ci]);
-        sp.cnt[ci] = (unsigned char)c;
-        for (int j = 0; j < c; j++) sp.radix[k++] = (unsigned char)kRadices[ci];
+    // the device runs passes in CFFT_EXEC_ORDER (odd radices first)
+    radix_counts(rad, sp.cnt);
+    {
+        auto ex = exec_order(rad);
+        if ((int)ex.size() != sp.np) return fail(CFFT_ERR_UNSUPPORTED, "radix outside the codelet set");
+        for (int i = 0; i < sp.np; i++) sp.radix[i] = (unsigned char)ex[i];
     }
-    if (k != sp.np) return fail(CFFT_ERR_UNSUPPORTED, "radix outside the codelet set");
     sp.G = std::max(1, wave_G(rad, L, CFFT_THREADS));
     // warp-synchronous mode when a warp can own whole sub-transforms and
     // there are enough of them to occupy every warp of the block
@@ -435,19 +453,28 @@ static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, 
     if (gw > 1 << 16) gw = 1 << 16;
     sp.Gwarp = 0;
     if (gw >= 1 && count >= (int64_t)(CFFT_THREADS / 32) * gw / 2) sp.Gwarp = gw;
-    if (L <= 1) { sp.tw = nullptr; return CFFT_OK; }
+    if (L <= 1) { sp.tw = nullptr; sp.twlen = 0; return CFFT_OK; }
+    // per-pass blocks: pass (r, s), n1 = L/(s r): tw[off + (j-1) n1 + q] = w_L^(j q s)
+    std::vector<double2> w;
+    {
+        int64_t s = 1;
+        for (int i = 0; i < sp.np; i++) {
+            const int r = sp.radix[i];
+            const int64_t n1 = L / (s * r);
+            for (int j = 1; j < r; j++)
+                for (int64_t q = 0; q < n1; q++) w.push_back(omega((int64_t)j * q * s, L, -1));
+            s *= r;
+        }
+    }
+    sp.twlen = (int)w.size();
     void* d = nullptr;
     int rc;
+    if (w.empty()) { sp.tw = nullptr; return CFFT_OK; }
     if (P->dtype == CFFT_C128) {
-        std::vector<double2> t(L);
-        for (int64_t m = 0; m < L; m++) t[m] = omega(m, L, -1);
-        rc = dev_upload(P, t.data(), t.size() * sizeof(double2), &d);
+        rc = dev_upload(P, w.data(), w.size() * sizeof(double2), &d);
     } else {
-        std::vector<float2> t(L);
-        for (int64_t m = 0; m < L; m++) {
-            double2 w = omega(m, L, -1);
-            t[m] = make_float2((float)w.x, (float)w.y);
-        }
+        std::vector<float2> t(w.size());
+        for (size_t m = 0; m < w.size(); m++) t[m] = make_float2((float)w[m].x, (float)w[m].y);
         rc = dev_upload(P, t.data(), t.size() * sizeof(float2), &d);
     }
     sp.tw = d;
@@ -634,8 +661,17 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.in_sel = 0;
         s.out_sel = 1;
         s.fn = cfft_static_four(P->dtype, sh.N1, sh.N2, sh.C, kp.pa.cnt, kp.pc.cnt);
-        if (s.fn) P->desc += "+static";
-        else s.fn = cfft_kernel_for(MODE_FOUR, P->dtype);
+        if (s.fn) {
+            P->desc += "+static";
+        } else if (kp.pa.Gwarp > 0 && kp.pc.Gwarp > 0) {
+            s.fn = cfft_kernel_for(MODE_FOUR_WARP, P->dtype);
+            P->desc += "+warp";
+        } else {
+            // one team kind per kernel: both sub-plans block-wide
+            s.fn = cfft_kernel_for(MODE_FOUR, P->dtype);
+            s.kp.pa.Gwarp = 0;
+            s.kp.pc.Gwarp = 0;
+        }
         CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, sh.C));
         {
             int nclusters = 0;
