@@ -34,7 +34,7 @@ from ._lib import (BACKWARD, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERS
 FLAG = int
 PLANNER_DEFAULT = NO_FLAG
 
-__all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache",
+__all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache", "Batch",
            "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
            "describe_strategy", "version"]
 
@@ -243,6 +243,55 @@ def mul_(y, p: Spell, x):
     r = _run(x, FORWARD, p.flag)
     np.copyto(y, r)
     return y
+
+
+class Batch:
+    """Mixed-length batch (the batched form): transforms packed back to back.
+
+    ``Batch(lengths, dtype)`` plans every distinct length once;
+    ``b.execute(x)`` runs the whole batch on a CUDA torch tensor holding the
+    packed transforms (1-D, ``sum(lengths)`` elements) as one graph launch on
+    torch's current stream and returns the packed result.
+    """
+
+    def __init__(self, lengths, dtype=np.complex64, flags: int = 0):
+        import ctypes as _ct
+        self.lengths = [int(n) for n in lengths]
+        self.dtype_code = _dtype_code(dtype)
+        arr = (_ct.c_int64 * len(self.lengths))(*self.lengths)
+        h = _ct.c_void_p()
+        check(_lib.LIB.cfft_batch_create(_ct.byref(h), len(self.lengths), arr, self.dtype_code, int(flags)))
+        self.handle = h
+        self.total = int(_lib.LIB.cfft_batch_elements(h))
+        self.offsets = np.concatenate([[0], np.cumsum(self.lengths)[:-1]]).astype(np.int64)
+
+    def launches(self) -> int:
+        return int(_lib.LIB.cfft_batch_launches(self.handle))
+
+    def execute(self, x, direction: int = FORWARD, out=None):
+        import torch
+        if not (_is_torch(x) and x.is_cuda and x.dim() == 1 and x.numel() == self.total):
+            raise ValueError(f"expected a 1-D CUDA tensor of {self.total} elements")
+        if _dtype_code(x.dtype) != self.dtype_code:
+            raise TypeError("element type does not match the batch")
+        xc = x.contiguous()
+        y = torch.empty_like(xc) if out is None else out
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+        check(_lib.LIB.cfft_batch_execute(self.handle, ctypes.c_void_p(xc.data_ptr()),
+                                          ctypes.c_void_p(y.data_ptr()), int(direction),
+                                          ctypes.c_void_p(stream)))
+        return y
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.LIB.cfft_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def empty_cache() -> None:

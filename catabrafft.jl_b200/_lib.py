@@ -32,6 +32,11 @@ SIGNATURES = {
     "cfft_plan_launches": (_ci, [_vp]),
     "cfft_version": (_ci, []),
     "cfft_fft_twopass_noalloc": (_ci, [_i64, _i64, _ci, _vp, _vp, _ci, _vp]),
+    "cfft_batch_create": (_ci, [ctypes.POINTER(_vp), _i64, ctypes.POINTER(_i64), _ci, _ci]),
+    "cfft_batch_execute": (_ci, [_vp, _vp, _vp, _ci, _vp]),
+    "cfft_batch_destroy": (_ci, [_vp]),
+    "cfft_batch_elements": (_i64, [_vp]),
+    "cfft_batch_launches": (_ci, [_vp]),
 }
 
 

@@ -83,6 +83,10 @@ __device__ __forceinline__ float2 apply_tw(float2 v, const TwoLevel& t, unsigned
     return e ? fromd<float2>(cmul(tod(v), tw_two(t, e))) : v;
 }
 
+// block index within this parameter block's launch (batched launches run many
+// parameter blocks, each owning a contiguous range of blocks from p.blk0)
+__device__ __forceinline__ int block_id(const KParams& p) { return (int)blockIdx.x - p.blk0; }
+
 template <typename V> __device__ __forceinline__ V load_in(const KParams& p, V v) {
     return p.dir ? conjv(v) : v;
 }
@@ -263,7 +267,7 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
     const int T = blockDim.x, tid = opaque_tid();
     V* buf = (V*)smem;
     V* xs = buf + (size_t)p.V * p.PC;
-    const int t0 = blockIdx.x * p.V;
+    const int t0 = block_id(p) * p.V;
     const int nrows = min(p.V, p.batch - t0);
     if (nrows <= 0) return;
     const V* in = (const V*)p.in + (long long)t0 * p.in_dist;
@@ -676,7 +680,7 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
     const int C = K::C(p);
     cg::cluster_group cl = cg::this_cluster();
     const unsigned c = (C > 1) ? cl.block_rank() : 0;
-    const int t = blockIdx.x / C;
+    const int t = block_id(p) / C;
     if (t >= p.batch) return;             // uniform across the cluster
     const int T = blockDim.x, tid = opaque_tid();
     const int N1 = K::N1(p), N2 = K::N2(p);
@@ -712,7 +716,8 @@ template <typename V, int EMAX>
 __device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* smem) {
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V;
-    const int t = blockIdx.x / tiles, c0 = (blockIdx.x - t * tiles) * p.V;
+    const int b = block_id(p);
+    const int t = b / tiles, c0 = (b - t * tiles) * p.V;
     if (t >= p.batch) return;
     V* buf = (V*)smem;
     const V* in = (const V*)p.in + (long long)t * p.in_dist;
@@ -747,7 +752,8 @@ template <typename V, int EMAX>
 __device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* smem) {
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N1 / p.V;
-    const int t = blockIdx.x / tiles, r0 = (blockIdx.x - t * tiles) * p.V;
+    const int b = block_id(p);
+    const int t = b / tiles, r0 = (b - t * tiles) * p.V;
     if (t >= p.batch) return;
     V* buf = (V*)smem;
     const V* in = (const V*)p.in + (long long)t * p.in_dist;

@@ -62,5 +62,20 @@ struct KParams {
     double scale;                 // 1/nx for dir 1, else 1
     // multiply-shift reciprocals (see fdiv) of the layout's divisors
     unsigned long long mW, mN2, mR1, mX, mM, mL, mV;
+    int blk0;                     // first block of this parameter block in its launch
+    unsigned char in_user, out_user;  // batched launches: in/out relative to the caller's buffers
+    unsigned char pad_[2];
+    long long in_off, out_off;    // batched launches: element offsets added to the bases
+};
+
+// One launch of the batched executor: parameter blocks in device memory and,
+// per block of the grid, the index of its parameter block.
+struct BatchLaunch {
+    const KParams* desc;
+    const int* block_desc;
+    const void* in_base;
+    void* out_base;
+    int dir;
+    int pad_;
 };
 

@@ -29,6 +29,92 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_rowpass(K
     rowpass_body<V, EMAX>(p, smem);
 }
 
+// ---- batched entry points: each block finds its parameter block, stages it
+// in shared memory with the launch's base pointers and direction applied, and
+// runs the same body as the single-plan kernels.
+template <typename V>
+__device__ __forceinline__ const KParams& stage_params(const BatchLaunch& L, KParams* sp) {
+    if (threadIdx.x == 0) {
+        KParams p = L.desc[L.block_desc[blockIdx.x]];
+        if (p.in_user) p.in = (const V*)L.in_base + p.in_off;
+        if (p.out_user) p.out = (V*)L.out_base + p.out_off;
+        p.dir = L.dir;
+        if (L.dir != 1) p.scale = 1.0;
+        *sp = p;
+    }
+    __syncthreads();
+    return *sp;
+}
+template <typename V, int EMAX>
+__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_rows(BatchLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ KParams sp;
+    rows_body<V, EMAX>(stage_params<V>(L, &sp), smem);
+}
+template <typename V, int EMAX, class K>
+__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_four(BatchLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ KParams sp;
+    four_body<V, EMAX, K>(stage_params<V>(L, &sp), smem);
+}
+
+template <typename V, int EMAX>
+__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_colpass(BatchLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ KParams sp;
+    colpass_body<V, EMAX>(stage_params<V>(L, &sp), smem);
+}
+template <typename V, int EMAX>
+__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_rowpass(BatchLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ KParams sp;
+    rowpass_body<V, EMAX>(stage_params<V>(L, &sp), smem);
+}
+
+const void* cfft_batch_kernel_for(int mode, int dtype) {
+    if (dtype == CFFT_DT_C128) {
+        switch (mode) {
+            case MODE_ROWS: return (const void*)kb_rows<double2, CFFT_EMAX>;
+            case MODE_FOUR: return (const void*)kb_four<double2, CFFT_EMAX, DynK<0>>;
+            case MODE_FOUR_WARP: return (const void*)kb_four<double2, CFFT_EMAX, DynK<1>>;
+            case MODE_COLPASS: return (const void*)kb_colpass<double2, CFFT_EMAX>;
+            case MODE_ROWPASS: return (const void*)kb_rowpass<double2, CFFT_EMAX>;
+        }
+    } else {
+        switch (mode) {
+            case MODE_ROWS: return (const void*)kb_rows<float2, CFFT_EMAX>;
+            case MODE_FOUR: return (const void*)kb_four<float2, CFFT_EMAX, DynK<0>>;
+            case MODE_FOUR_WARP: return (const void*)kb_four<float2, CFFT_EMAX, DynK<1>>;
+            case MODE_COLPASS: return (const void*)kb_colpass<float2, CFFT_EMAX>;
+            case MODE_ROWPASS: return (const void*)kb_rowpass<float2, CFFT_EMAX>;
+        }
+    }
+    return nullptr;
+}
+
+cudaError_t cfft_launch_batch(const void* f, const BatchLaunch& L, unsigned grid, size_t smem,
+                              int cluster, cudaStream_t stream) {
+    if (!f) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(CFFT_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    if (cluster > 1) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    void* args[] = {(void*)&L};
+    cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
+
 const void* cfft_kernel_for(int mode, int dtype) {
     if (dtype == CFFT_DT_C128) {
         switch (mode) {
@@ -94,8 +180,12 @@ cudaError_t cfft_prepare_fn(const void* f, size_t smem, int cluster) {
     if (!f) return cudaErrorInvalidValue;
     // always the device maximum: a smaller value set for one plan would break
     // another plan that shares the kernel and needs more
-    if (smem > 232448) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return e;
+    const size_t cap = 232448 - fa.sharedSizeBytes;   // 227 KB per block minus static
+    if (smem > cap) return cudaErrorInvalidValue;
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
     if (e != cudaSuccess) return e;
     if (cluster > 8) {
         e = cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

@@ -20,5 +20,15 @@ cudaError_t cfft_prepare_fn(const void* fn, size_t smem, int cluster);
 cudaError_t cfft_launch_fn(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
                            int cluster, cudaStream_t stream);
 cudaError_t cfft_max_active_clusters_fn(const void* fn, int threads, size_t smem, int cluster, int* out);
+// batched (descriptor-driven) kernels
+const void* cfft_batch_kernel_for(int mode, int dtype);
+cudaError_t cfft_launch_batch(const void* fn, const BatchLaunch& L, unsigned grid, size_t smem,
+                              int cluster, cudaStream_t stream);
+// convolution tables on the device (tables.cu)
+cudaError_t cfft_gen_chirp(double2* ch, long long n, cudaStream_t st);
+cudaError_t cfft_gen_bluestein_b(double2* b, const double2* ch, long long n, long long M, cudaStream_t st);
+cudaError_t cfft_gen_rader_b(double2* b, const int* iperm, long long n, long long M, int exact,
+                             double2 winv, cudaStream_t st);
+cudaError_t cfft_scale(double2* v, long long M, double s, cudaStream_t st);
 // set the thread-local text returned by cfft_last_error() (fixed buffer)
 void cfft_set_last_error(const char* msg);

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -233,6 +234,19 @@ struct Shape {
     double score = 0;
 };
 
+// Reference-counted device buffer.  Tables that depend only on a length (sub-
+// transform twiddles, four-step tables, convolution spectra) are shared
+// through a process-wide cache; plans hold references, so dropping the cache
+// (cfft_empty_cache) never frees a table a live plan still uses.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+using DevPtr = std::shared_ptr<DevBuf>;
+
 struct cfft_plan_s {
     int64_t n = 0, batch = 0;
     int dtype = 0, flags = 0;
@@ -243,6 +257,8 @@ struct cfft_plan_s {
     void* scratch[2] = {nullptr, nullptr};
     size_t scratch_bytes = 0;
     std::vector<void*> allocs;
+    std::vector<DevPtr> tables;  // shared, cached tables
+    bool shared_scratch = false; // scratch provided by a batch (not allocated here)
     int device = 0;
     // host-buffer pipeline (created on first cfft_execute_host)
     std::mutex host_mu;
@@ -433,6 +449,57 @@ static int dev_upload(cfft_plan_s* P, const void* h, size_t bytes, void** d) {
     CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
     return CFFT_OK;
 }
+static std::mutex g_tab_mu;
+static std::map<std::string, DevPtr> g_tables;
+
+static int dev_alloc(size_t bytes, DevPtr* out) {
+    auto b = std::make_shared<DevBuf>();
+    cudaError_t e = cudaMalloc(&b->p, bytes);
+    if (e != cudaSuccess) {
+        b->p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? CFFT_ERR_NOMEM : CFFT_ERR_CUDA,
+                    std::string("table allocation: ") + cudaGetErrorString(e));
+    }
+    b->bytes = bytes;
+    *out = b;
+    return CFFT_OK;
+}
+// cached table: look `key` up (per device); on a miss build the host image
+// with `make` and upload it
+template <class F>
+static int cached_table(cfft_plan_s* P, const std::string& key0, F make, const void** out) {
+    const std::string key = std::to_string(P->device) + "/" + key0;
+    {
+        std::lock_guard<std::mutex> lk(g_tab_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) {
+            P->tables.push_back(it->second);
+            *out = it->second->p;
+            return CFFT_OK;
+        }
+    }
+    std::vector<unsigned char> img;
+    make(img);
+    DevPtr b;
+    int rc = dev_alloc(img.size(), &b);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(b->p, img.data(), img.size(), cudaMemcpyHostToDevice));
+    {
+        std::lock_guard<std::mutex> lk(g_tab_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) b = it->second;   // another thread won the race
+        else g_tables[key] = b;
+    }
+    P->tables.push_back(b);
+    *out = b->p;
+    return CFFT_OK;
+}
+template <class T> static void put(std::vector<unsigned char>& img, const std::vector<T>& v) {
+    img.resize(v.size() * sizeof(T));
+    memcpy(img.data(), v.data(), img.size());
+}
+
 static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, int64_t count,
                         SubPlan& sp) {
     memset(&sp, 0, sizeof sp);
@@ -455,44 +522,45 @@ static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, 
     if (gw >= 1 && count >= (int64_t)(CFFT_THREADS / 32) * gw / 2) sp.Gwarp = gw;
     if (L <= 1) { sp.tw = nullptr; sp.twlen = 0; return CFFT_OK; }
     // per-pass blocks: pass (r, s), n1 = L/(s r): tw[off + (j-1) n1 + q] = w_L^(j q s)
-    std::vector<double2> w;
-    {
+    sp.twlen = (int)twiddle_len(L, rad);
+    if (sp.twlen == 0) { sp.tw = nullptr; return CFFT_OK; }
+    std::string key = "tw/" + std::to_string(P->dtype) + "/" + std::to_string(L) + "/" + join(rad);
+    const int np = sp.np;
+    unsigned char radix[CFFT_MAXP];
+    memcpy(radix, sp.radix, sizeof radix);
+    const int dtype = P->dtype;
+    return cached_table(P, key, [&](std::vector<unsigned char>& img) {
+        std::vector<double2> w;
         int64_t s = 1;
-        for (int i = 0; i < sp.np; i++) {
-            const int r = sp.radix[i];
+        for (int i = 0; i < np; i++) {
+            const int r = radix[i];
             const int64_t n1 = L / (s * r);
             for (int j = 1; j < r; j++)
                 for (int64_t q = 0; q < n1; q++) w.push_back(omega((int64_t)j * q * s, L, -1));
             s *= r;
         }
-    }
-    sp.twlen = (int)w.size();
-    void* d = nullptr;
-    int rc;
-    if (w.empty()) { sp.tw = nullptr; return CFFT_OK; }
-    if (P->dtype == CFFT_C128) {
-        rc = dev_upload(P, w.data(), w.size() * sizeof(double2), &d);
-    } else {
-        std::vector<float2> t(w.size());
-        for (size_t m = 0; m < w.size(); m++) t[m] = make_float2((float)w[m].x, (float)w[m].y);
-        rc = dev_upload(P, t.data(), t.size() * sizeof(float2), &d);
-    }
-    sp.tw = d;
-    return rc;
+        if (dtype == CFFT_C128) {
+            put(img, w);
+        } else {
+            std::vector<float2> t(w.size());
+            for (size_t m = 0; m < w.size(); m++) t[m] = make_float2((float)w[m].x, (float)w[m].y);
+            put(img, t);
+        }
+    }, &sp.tw);
 }
 static int make_twolevel(cfft_plan_s* P, int64_t N, TwoLevel& t) {
     const int bits = twolevel_bits(N);
-    int64_t lo_n = 1LL << bits, hi_n = (N + lo_n - 1) / lo_n + 1;
-    std::vector<double2> lo(lo_n), hi(hi_n);
-    for (int64_t a = 0; a < lo_n; a++) lo[a] = omega(a, N, -1);
-    for (int64_t b = 0; b < hi_n; b++) hi[b] = omega(b * lo_n, N, -1);
-    void *dl, *dh;
-    int rc = dev_upload(P, lo.data(), lo.size() * sizeof(double2), &dl);
+    const int64_t lo_n = 1LL << bits, hi_n = (N + lo_n - 1) / lo_n + 1;
+    const void* d = nullptr;
+    int rc = cached_table(P, "tl/" + std::to_string(N), [&](std::vector<unsigned char>& img) {
+        std::vector<double2> v(lo_n + hi_n);
+        for (int64_t a = 0; a < lo_n; a++) v[a] = omega(a, N, -1);
+        for (int64_t b = 0; b < hi_n; b++) v[lo_n + b] = omega(b * lo_n, N, -1);
+        put(img, v);
+    }, &d);
     if (rc) return rc;
-    rc = dev_upload(P, hi.data(), hi.size() * sizeof(double2), &dh);
-    if (rc) return rc;
-    t.lo = (const double2*)dl;
-    t.hi = (const double2*)dh;
+    t.lo = (const double2*)d;
+    t.hi = (const double2*)d + lo_n;
     t.bits = bits;
     t.N = (int)N;
     return CFFT_OK;
@@ -503,92 +571,121 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
                         int64_t nbatch = -1);
 static void plan_free(cfft_plan_s* P);
 
-// spectrum = FFT_M(b) / M in FP64 using this library's own C128 path
-static int conv_spectrum(cfft_plan_s* P, int64_t M, const std::vector<double2>& b, const double2** out) {
-    cfft_plan_s sub;
-    sub.n = M;
-    sub.batch = 1;
-    sub.dtype = CFFT_C128;
-    sub.flags = 0;
-    auto cands = candidate_shapes(M, CFFT_C128, 1);
-    if (cands.empty()) return fail(CFFT_ERR_UNSUPPORTED, "no shape for convolution length");
-    int rc = CFFT_ERR_UNSUPPORTED;
-    for (auto& c : cands) {
-        rc = plan_build(&sub, c);
-        if (rc == CFFT_OK) break;
-        plan_free(&sub);
+static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dtype, int flags);
+
+// cached table built on the device by `build(dptr)` on a miss
+template <class F>
+static int cached_dev_table(cfft_plan_s* P, const std::string& key0, size_t bytes, F build,
+                            const void** out) {
+    const std::string key = std::to_string(P->device) + "/" + key0;
+    {
+        std::lock_guard<std::mutex> lk(g_tab_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) {
+            P->tables.push_back(it->second);
+            *out = it->second->p;
+            return CFFT_OK;
+        }
     }
+    DevPtr b;
+    int rc = dev_alloc(bytes, &b);
     if (rc) return rc;
-    void *din = nullptr, *dout = nullptr;
-    rc = dev_upload(P, b.data(), M * sizeof(double2), &din);
-    if (rc) { plan_free(&sub); return rc; }
-    CUDA_TRY(cudaMalloc(&dout, M * sizeof(double2)));
-    P->allocs.push_back(dout);
-    rc = plan_execute(&sub, din, dout, CFFT_FORWARD, 0);
-    cudaError_t e = cudaDeviceSynchronize();
-    plan_free(&sub);
+    rc = build(b->p);
     if (rc) return rc;
-    if (e != cudaSuccess) return fail(CFFT_ERR_CUDA, std::string("spectrum: ") + cudaGetErrorString(e));
-    std::vector<double2> h(M);
-    CUDA_TRY(cudaMemcpy(h.data(), dout, M * sizeof(double2), cudaMemcpyDeviceToHost));
-    for (auto& v : h) { v.x /= (double)M; v.y /= (double)M; }
-    CUDA_TRY(cudaMemcpy(dout, h.data(), M * sizeof(double2), cudaMemcpyHostToDevice));
-    *out = (const double2*)dout;
+    CUDA_TRY(cudaStreamSynchronize(0));
+    {
+        std::lock_guard<std::mutex> lk(g_tab_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) b = it->second;
+        else g_tables[key] = b;
+    }
+    P->tables.push_back(b);
+    *out = b->p;
     return CFFT_OK;
+}
+
+// smooth FP64 plans (batch 1) that transform convolution kernel vectors,
+// cached per (device, M)
+static std::mutex g_spec_mu;
+static std::map<std::pair<int, int64_t>, cfft_plan_s*> g_spec_plans;
+static int spectrum_plan(int dev, int64_t M, cfft_plan_s** out) {
+    std::lock_guard<std::mutex> lk(g_spec_mu);
+    auto it = g_spec_plans.find({dev, M});
+    if (it != g_spec_plans.end()) { *out = it->second; return CFFT_OK; }
+    cfft_plan_s* S = nullptr;
+    int rc = plan_create_impl(&S, M, 1, CFFT_C128, CFFT_NO_FLAG);
+    if (rc) return rc;
+    g_spec_plans[{dev, M}] = S;
+    *out = S;
+    return CFFT_OK;
+}
+// spectrum = FFT_M(b') / M in FP64, b' generated in place by `gen`
+template <class G>
+static int conv_spectrum(cfft_plan_s* P, const std::string& key, int64_t M, G gen, const double2** out) {
+    cfft_plan_s* S = nullptr;
+    int rc = spectrum_plan(P->device, M, &S);
+    if (rc) return rc;
+    const void* d = nullptr;
+    rc = cached_dev_table(P, key, (size_t)M * sizeof(double2), [&](void* dp) -> int {
+        double2* v = (double2*)dp;
+        CUDA_TRY(gen(v));
+        int r = plan_execute(S, v, v, CFFT_FORWARD, 0);
+        if (r) return r;
+        CUDA_TRY(cfft_scale(v, M, 1.0 / (double)M, 0));
+        return CFFT_OK;
+    }, &d);
+    *out = (const double2*)d;
+    return rc;
 }
 
 static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp) {
     const int64_t n = P->n, M = sh.M;
-    std::vector<double2> b(M, make_double2(0, 0));
+    const std::string tag = std::to_string(n) + "/" + std::to_string(M);
     if (sh.conv == CONV_RADER) {
-        const int64_t L = n - 1, g = primitive_root(n), ginv = powmod(g, n - 2, n);
-        std::vector<int> perm(L), iperm(L);
-        int64_t a = 1, c = 1;
-        for (int64_t i = 0; i < L; i++) {
-            perm[i] = (int)a;
-            iperm[i] = (int)c;
-            a = (int64_t)(((__int128)a * g) % n);
-            c = (int64_t)(((__int128)c * ginv) % n);
-        }
-        // W[m] = w^(-g^-m): the reference's twiddles (prime.jl:36-37) or exact
-        std::vector<double2> W(L);
-        if (P->flags & CFFT_EXACT_TWIDDLES) {
-            for (int64_t m = 0; m < L; m++) W[m] = omega(iperm[m], n, -1);
-        } else {
-            double2 w = omega(1, n, +1);                 // cispi(2/n)
-            {
-                // cispi(T(2/n)) evaluates at the rounded argument 2/n
-                double arg = 2.0 / (double)n;            // in units of pi
-                long double x = 3.141592653589793238462643383279502884L * (long double)arg;
-                w = make_double2((double)cosl(x), (double)sinl(x));
+        const int64_t L = n - 1;
+        const void* dperm = nullptr;
+        // perm[j] = g^j mod n and iperm[j] = g^-j mod n (prime.jl:9-33), one buffer
+        int rc = cached_table(P, "pm/" + std::to_string(n), [&](std::vector<unsigned char>& img) {
+            const int64_t g = primitive_root(n), ginv = powmod(g, n - 2, n);
+            std::vector<int> v(2 * L);
+            int64_t a = 1, c = 1;
+            for (int64_t i = 0; i < L; i++) {
+                v[i] = (int)a;
+                v[L + i] = (int)c;
+                a = (int64_t)(((__int128)a * g) % n);
+                c = (int64_t)(((__int128)c * ginv) % n);
             }
-            double2 winv = julia_inv(w);
-            for (int64_t m = 0; m < L; m++) W[m] = pow_by_squaring(winv, iperm[m]);
+            put(img, v);
+        }, &dperm);
+        if (rc) return rc;
+        kp.perm = (const int*)dperm;
+        kp.iperm = (const int*)dperm + L;
+        // W[m] = w^(-g^-m): the reference's recurrence (prime.jl:36-37) or exact
+        const int exact = (P->flags & CFFT_EXACT_TWIDDLES) ? 1 : 0;
+        double2 winv = make_double2(1, 0);
+        if (!exact) {
+            // cispi(T(2/n)) at the rounded argument 2/n, then Julia's inv
+            const double arg = 2.0 / (double)n;
+            const long double x = 3.141592653589793238462643383279502884L * (long double)arg;
+            winv = julia_inv(make_double2((double)cosl(x), (double)sinl(x)));
         }
-        for (int64_t m = 0; m < L; m++) b[m] = W[m];
-        for (int64_t m = 1; m < L; m++) b[M - L + m] = W[m];
-        void *dp, *di;
-        int rc = dev_upload(P, perm.data(), L * sizeof(int), &dp);
-        if (rc) return rc;
-        rc = dev_upload(P, iperm.data(), L * sizeof(int), &di);
-        if (rc) return rc;
-        kp.perm = (const int*)dp;
-        kp.iperm = (const int*)di;
-    } else {
-        // chirp[j] = exp(-i pi j^2 / n); b[m] = conj(chirp[|m|])
-        std::vector<double2> ch(n);
-        for (int64_t j = 0; j < n; j++) {
-            int64_t e = (int64_t)(((__int128)j * j) % (2 * n));
-            ch[j] = omega(e, 2 * n, -1);
-        }
-        for (int64_t m = 0; m < n; m++) b[m] = make_double2(ch[m].x, -ch[m].y);
-        for (int64_t m = 1; m < n; m++) b[M - m] = make_double2(ch[m].x, -ch[m].y);
-        void* dc;
-        int rc = dev_upload(P, ch.data(), n * sizeof(double2), &dc);
-        if (rc) return rc;
-        kp.chirp = (const double2*)dc;
+        const int* iperm = kp.iperm;
+        return conv_spectrum(P, "sr/" + tag + "/" + std::to_string(exact), M, [&](double2* v) {
+            return cfft_gen_rader_b(v, iperm, n, M, exact, winv, 0);
+        }, &kp.spec);
     }
-    return conv_spectrum(P, M, b, &kp.spec);
+    // Bluestein: chirp[j] = exp(-i pi j^2 / n); b'[m] = conj(chirp[|m|])
+    const void* dch = nullptr;
+    int rc = cached_dev_table(P, "ch/" + std::to_string(n), (size_t)n * sizeof(double2), [&](void* dp) -> int {
+        CUDA_TRY(cfft_gen_chirp((double2*)dp, n, 0));
+        return CFFT_OK;
+    }, &dch);
+    if (rc) return rc;
+    kp.chirp = (const double2*)dch;
+    const double2* ch = kp.chirp;
+    return conv_spectrum(P, "sb/" + tag, M, [&](double2* v) {
+        return cfft_gen_bluestein_b(v, ch, n, M, 0);
+    }, &kp.spec);
 }
 
 static int plan_build(cfft_plan_s* P, const Shape& sh) {
@@ -711,9 +808,11 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     chunk = std::min<int64_t>(chunk, P->batch);
     P->chunk = chunk;
     P->scratch_bytes = (size_t)chunk * M * e;
-    for (int i = 0; i < nscr; i++) {
-        CUDA_TRY(cudaMalloc(&P->scratch[i], P->scratch_bytes));
-        P->allocs.push_back(P->scratch[i]);
+    if (!P->shared_scratch) {
+        for (int i = 0; i < nscr; i++) {
+            CUDA_TRY(cudaMalloc(&P->scratch[i], P->scratch_bytes));
+            P->allocs.push_back(P->scratch[i]);
+        }
     }
     auto col = [&](int pre, int in_sel, int out_sel) {
         Stage s;
@@ -783,6 +882,7 @@ static void plan_free(cfft_plan_s* P) {
     }
     for (void* p : P->allocs) cudaFree(p);
     P->allocs.clear();
+    P->tables.clear();
     P->stages.clear();
     P->scratch[0] = P->scratch[1] = nullptr;
 }
@@ -900,6 +1000,278 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
     return CFFT_OK;
 }
 
+
+// ------------------------------------------------------------ batched form
+// Many transforms of mixed lengths packed back to back.  Every transform gets
+// a parameter block in device memory; transforms whose plan is a single
+// kernel (rows or cluster four-step) are grouped by kernel variant, cluster
+// size and shared-memory class, and each group runs as one launch whose
+// blocks look up their parameter block.  Transforms that need two HBM passes
+// run through their plan's launches on a scratch shared by the whole batch.
+// Groups are ordered largest transform first (longest-processing-time
+// order) so the block scheduler balances the tail.  The whole sequence is
+// captured once into a CUDA graph per (input, output, direction).
+struct cfft_batch_s {
+    int dtype = 0, flags = 0, device = 0;
+    int64_t count = 0, total = 0;
+    std::vector<int64_t> len, off;
+    std::map<int64_t, cfft_plan_s*> plans;
+    struct Group {
+        const void* fn = nullptr;
+        int cluster = 1;
+        size_t smem = 0;
+        unsigned grid = 0;
+        KParams* d_desc = nullptr;
+        int* d_map = nullptr;
+        int ndesc = 0;
+        double cost = 0;
+    };
+    std::vector<Group> groups;   // single-kernel transforms
+    std::vector<Group> passes;   // two-pass transforms, chunk by chunk, pass by pass
+    void* scratch[2] = {nullptr, nullptr};
+    std::vector<void*> allocs;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void* g_in = nullptr;
+    void* g_out = nullptr;
+    int g_dir = -1;
+    int launches = 0;
+    std::mutex mu;
+};
+
+static void batch_free(cfft_batch_s* B) {
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    B->gexec = nullptr;
+    if (B->cap) cudaStreamDestroy(B->cap);
+    B->cap = nullptr;
+    for (auto& kv : B->plans) {
+        plan_free(kv.second);
+        delete kv.second;
+    }
+    B->plans.clear();
+    for (void* q : B->allocs) cudaFree(q);
+    B->allocs.clear();
+}
+
+// launches are grouped by how many CTAs fit an SM (two below ~113 KB of
+// shared memory, one above); a group runs with its largest member's size
+static int smem_class(size_t smem) { return smem <= (size_t)112 * 1024 ? 0 : 1; }
+// one launch: parameter blocks (largest first) and the block -> block map
+template <class ItemT>
+static int make_group(cfft_batch_s* B, const void* fn, int cluster, std::vector<ItemT>& items,
+                      cfft_batch_s::Group& g) {
+    std::stable_sort(items.begin(), items.end(), [](const ItemT& a, const ItemT& b) { return a.cost > b.cost; });
+    g.fn = fn;
+    g.cluster = cluster;
+    g.smem = 0;
+    for (auto& it : items) g.smem = std::max(g.smem, it.smem);
+    std::vector<KParams> desc;
+    std::vector<int> map;
+    for (auto& it : items) {
+        KParams kp = it.kp;
+        kp.blk0 = (int)map.size();
+        int nb = 1;
+        if (kp.mode == MODE_FOUR) nb = kp.C;
+        else if (kp.mode == MODE_COLPASS) nb = kp.N2 / kp.V;
+        else if (kp.mode == MODE_ROWPASS) nb = kp.N1 / kp.V;
+        for (int b = 0; b < nb; b++) map.push_back((int)desc.size());
+        desc.push_back(kp);
+        g.cost += it.cost;
+    }
+    g.ndesc = (int)desc.size();
+    g.grid = (unsigned)map.size();
+    void *dd = nullptr, *dm = nullptr;
+    CUDA_TRY(cudaMalloc(&dd, desc.size() * sizeof(KParams)));
+    B->allocs.push_back(dd);
+    CUDA_TRY(cudaMalloc(&dm, map.size() * sizeof(int)));
+    B->allocs.push_back(dm);
+    CUDA_TRY(cudaMemcpy(dd, desc.data(), desc.size() * sizeof(KParams), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(dm, map.data(), map.size() * sizeof(int), cudaMemcpyHostToDevice));
+    g.d_desc = (KParams*)dd;
+    g.d_map = (int*)dm;
+    CUDA_TRY(cfft_prepare_fn(g.fn, g.smem, g.cluster));
+    return CFFT_OK;
+}
+
+static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* lengths, int dtype, int flags) {
+    const size_t e = elem_bytes(dtype);
+    B->dtype = dtype;
+    B->flags = flags & CFFT_EXACT_TWIDDLES;
+    B->count = count;
+    cudaGetDevice(&B->device);
+    B->len.assign(lengths, lengths + count);
+    B->off.resize(count);
+    int64_t acc = 0;
+    for (int64_t i = 0; i < count; i++) {
+        if (lengths[i] < 1) return fail(CFFT_ERR_INVALID, "every length must be >= 1");
+        B->off[i] = acc;
+        acc += lengths[i];
+    }
+    B->total = acc;
+    // one plan per distinct length (batch 1, scratch shared by the batch)
+    for (int64_t n : B->len) {
+        if (B->plans.count(n)) continue;
+        if (n > (1LL << 26)) return fail(CFFT_ERR_UNSUPPORTED, "length above 2^26");
+        auto cands = candidate_shapes(n, dtype, 1);
+        cfft_plan_s* P = new cfft_plan_s();
+        P->n = n;
+        P->batch = 1;
+        P->dtype = dtype;
+        P->flags = B->flags;
+        P->device = B->device;
+        P->shared_scratch = true;
+        int rc = CFFT_ERR_UNSUPPORTED;
+        for (auto& c : cands) {
+            rc = plan_build(P, c);
+            if (rc == CFFT_OK) break;
+            plan_free(P);
+        }
+        if (rc) {
+            delete P;
+            return rc;
+        }
+        B->plans[n] = P;
+    }
+    // group single-kernel transforms; collect the two-pass ones
+    struct Item { int64_t idx; KParams kp; double cost; size_t smem; };
+    std::map<std::tuple<const void*, int, int>, std::vector<Item>> bins;
+    std::vector<int64_t> twopass;
+    for (int64_t i = 0; i < count; i++) {
+        cfft_plan_s* P = B->plans[B->len[i]];
+        const double cost = (double)P->shape.M * std::log2((double)std::max<int64_t>(2, P->shape.M));
+        if (P->stages.size() == 1 && (P->stages[0].kp.mode == MODE_ROWS || P->stages[0].kp.mode == MODE_FOUR)) {
+            KParams kp = P->stages[0].kp;
+            int kmode = kp.mode;
+            if (kp.mode == MODE_FOUR) {
+                if (kp.pa.Gwarp > 0 && kp.pc.Gwarp > 0) kmode = MODE_FOUR_WARP;
+                else kp.pa.Gwarp = kp.pc.Gwarp = 0;
+            }
+            kp.batch = 1;
+            kp.in_off = kp.out_off = B->off[i];
+            kp.in_user = kp.out_user = 1;
+            kp.in_dist = kp.out_dist = B->len[i];
+            kp.scale = 1.0 / (double)B->len[i];
+            const void* fn = cfft_batch_kernel_for(kmode, dtype);
+            bins[std::make_tuple(fn, P->stages[0].cluster, smem_class(P->stages[0].smem))]
+                .push_back({i, kp, cost, P->stages[0].smem});
+        } else {
+            twopass.push_back(i);
+        }
+    }
+    for (auto& kv : bins) {
+        cfft_batch_s::Group g;
+        int rc = make_group(B, std::get<0>(kv.first), std::get<1>(kv.first), kv.second, g);
+        if (rc) return rc;
+        B->groups.push_back(g);
+    }
+    // costliest groups first
+    std::stable_sort(B->groups.begin(), B->groups.end(),
+                     [](const cfft_batch_s::Group& a, const cfft_batch_s::Group& b) { return a.cost > b.cost; });
+
+    // two-pass transforms: chunks that fit a shared scratch; per chunk, pass k
+    // of every transform runs as one launch per shared-memory class
+    if (!twopass.empty()) {
+        std::stable_sort(twopass.begin(), twopass.end(), [&](int64_t a, int64_t b) { return B->len[a] > B->len[b]; });
+        size_t freeb = 0, totb = 0;
+        cudaMemGetInfo(&freeb, &totb);
+        size_t budget = std::min<size_t>((size_t)4 << 30, freeb / 4);
+        size_t need_max = 0;
+        for (int64_t i : twopass) {
+            cfft_plan_s* P = B->plans[B->len[i]];
+            need_max = std::max(need_max, (size_t)P->shape.M * e * (P->stages.size() > 2 ? 2 : 1));
+        }
+        budget = std::max(budget, need_max);
+        CUDA_TRY(cudaMalloc(&B->scratch[0], budget));
+        B->allocs.push_back(B->scratch[0]);
+        size_t used = 0;
+        std::vector<int64_t> chunk;
+        auto flush = [&]() -> int {
+            if (chunk.empty()) return CFFT_OK;
+            // scratch offsets (elements) per transform: S1, S2
+            std::map<int64_t, std::pair<int64_t, int64_t>> so;
+            int64_t cur = 0;
+            for (int64_t i : chunk) {
+                cfft_plan_s* P = B->plans[B->len[i]];
+                const int64_t M = P->shape.M;
+                so[i] = {cur, P->stages.size() > 2 ? cur + M : -1};
+                cur += M * (P->stages.size() > 2 ? 2 : 1);
+            }
+            for (int pass = 0; pass < 4; pass++) {
+                std::map<std::tuple<const void*, int, int>, std::vector<Item>> pb;
+                for (int64_t i : chunk) {
+                    cfft_plan_s* P = B->plans[B->len[i]];
+                    if (pass >= (int)P->stages.size()) continue;
+                    const Stage& st = P->stages[pass];
+                    KParams kp = st.kp;
+                    kp.batch = 1;
+                    kp.scale = 1.0 / (double)B->len[i];
+                    auto where = [&](int sel, const void** ptr, long long* off, unsigned char* user, long long* dist) {
+                        if (sel <= 1) { *ptr = nullptr; *off = B->off[i]; *user = 1; *dist = B->len[i]; }
+                        else {
+                            const int64_t o = (sel == 2) ? so[i].first : so[i].second;
+                            *ptr = (const char*)B->scratch[0] + (size_t)o * e;
+                            *off = 0; *user = 0; *dist = P->shape.M;
+                        }
+                    };
+                    const void* ip; const void* op;
+                    where(st.in_sel, &ip, &kp.in_off, &kp.in_user, &kp.in_dist);
+                    where(st.out_sel, &op, &kp.out_off, &kp.out_user, &kp.out_dist);
+                    kp.in = ip;
+                    kp.out = (void*)op;
+                    const double cost = (double)P->shape.M;
+                    pb[std::make_tuple(cfft_batch_kernel_for(kp.mode, dtype), 1, smem_class(st.smem))]
+                        .push_back({i, kp, cost, st.smem});
+                }
+                for (auto& kv : pb) {
+                    cfft_batch_s::Group g;
+                    int rc = make_group(B, std::get<0>(kv.first), 1, kv.second, g);
+                    if (rc) return rc;
+                    B->passes.push_back(g);
+                }
+            }
+            chunk.clear();
+            used = 0;
+            return CFFT_OK;
+        };
+        for (int64_t i : twopass) {
+            cfft_plan_s* P = B->plans[B->len[i]];
+            const size_t need = (size_t)P->shape.M * e * (P->stages.size() > 2 ? 2 : 1);
+            if (used + need > budget) {
+                int rc = flush();
+                if (rc) return rc;
+            }
+            chunk.push_back(i);
+            used += need;
+        }
+        int rc = flush();
+        if (rc) return rc;
+    }
+    (void)e;
+    CUDA_TRY(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
+    return CFFT_OK;
+}
+
+static int batch_enqueue(cfft_batch_s* B, const void* in, void* out, int dir, cudaStream_t st) {
+    int launches = 0;
+    for (auto* list : {&B->groups, &B->passes}) {
+        for (auto& g : *list) {
+            BatchLaunch L;
+            L.desc = g.d_desc;
+            L.block_desc = g.d_map;
+            L.in_base = in;
+            L.out_base = out;
+            L.dir = dir;
+            L.pad_ = 0;
+            cudaError_t ce = cfft_launch_batch(g.fn, L, g.grid, g.smem, g.cluster, st);
+            if (ce != cudaSuccess)
+                return fail(CFFT_ERR_CUDA, std::string("batched launch: ") + cudaGetErrorString(ce));
+            launches++;
+        }
+    }
+    B->launches = launches;
+    return CFFT_OK;
+}
+
 // ------------------------------------------------------------------- C ABI
 static std::mutex g_cache_mu;
 static std::map<std::tuple<int, int64_t, int64_t, int, int>, cfft_plan_s*> g_cache;
@@ -994,12 +1366,24 @@ int cfft_fft(int64_t n, int64_t batch, int dtype, int flags, const void* d_in, v
 }
 
 int cfft_empty_cache(void) {
-    std::lock_guard<std::mutex> lk(g_cache_mu);
-    for (auto& kv : g_cache) {
-        plan_free(kv.second);
-        delete kv.second;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        for (auto& kv : g_cache) {
+            plan_free(kv.second);
+            delete kv.second;
+        }
+        g_cache.clear();
     }
-    g_cache.clear();
+    {
+        std::lock_guard<std::mutex> lk(g_spec_mu);
+        for (auto& kv : g_spec_plans) {
+            plan_free(kv.second);
+            delete kv.second;
+        }
+        g_spec_plans.clear();
+    }
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    g_tables.clear();   // live plans keep their own references
     return CFFT_OK;
 }
 
@@ -1020,6 +1404,72 @@ int cfft_describe_strategy(int64_t n, int dtype, char* buf, int len) {
 int64_t cfft_plan_workspace_bytes(cfft_plan plan) {
     if (!plan) return -1;
     return (int64_t)plan->scratch_bytes * ((plan->scratch[1] != nullptr) ? 2 : (plan->scratch[0] ? 1 : 0));
+}
+
+
+int cfft_batch_create(cfft_batch* batch, int64_t count, const int64_t* lengths, int dtype, int flags) {
+    g_err[0] = 0;
+    if (!batch || !lengths || count < 1) return fail(CFFT_ERR_INVALID, "batch, lengths and count >= 1 required");
+    if (dtype != CFFT_C128 && dtype != CFFT_C64) return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128 or CFFT_C64");
+    cfft_batch_s* B = new cfft_batch_s();
+    int rc = batch_create_impl(B, count, lengths, dtype, flags);
+    if (rc) {
+        std::string keep = g_err;
+        batch_free(B);
+        delete B;
+        cfft_set_last_error(keep.c_str());
+        return rc;
+    }
+    *batch = B;
+    return CFFT_OK;
+}
+
+int cfft_batch_execute(cfft_batch batch, const void* d_in, void* d_out, int direction, void* stream) {
+    if (!batch || !d_in || !d_out) return fail(CFFT_ERR_INVALID, "null batch or buffer");
+    if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    cfft_batch_s* B = batch;
+    const size_t e = elem_bytes(B->dtype);
+    if (((uintptr_t)d_in % e) || ((uintptr_t)d_out % e))
+        return fail(CFFT_ERR_INVALID, "buffers must be aligned to the element size");
+    std::lock_guard<std::mutex> lk(B->mu);
+    if (!B->gexec || B->g_in != d_in || B->g_out != d_out || B->g_dir != direction) {
+        if (B->gexec) cudaGraphExecDestroy(B->gexec);
+        B->gexec = nullptr;
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
+        int rc = batch_enqueue(B, d_in, d_out, direction, B->cap);
+        cudaError_t ce = cudaStreamEndCapture(B->cap, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(CFFT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&B->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            B->gexec = nullptr;
+            return fail(CFFT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        }
+        B->g_in = d_in;
+        B->g_out = d_out;
+        B->g_dir = direction;
+    }
+    CUDA_TRY(cudaGraphLaunch(B->gexec, (cudaStream_t)stream));
+    return CFFT_OK;
+}
+
+int cfft_batch_destroy(cfft_batch batch) {
+    if (!batch) return fail(CFFT_ERR_INVALID, "null batch");
+    batch_free(batch);
+    delete batch;
+    return CFFT_OK;
+}
+
+int64_t cfft_batch_elements(cfft_batch batch) { return batch ? batch->total : -1; }
+
+int cfft_batch_launches(cfft_batch batch) {
+    if (!batch) return -1;
+    return (int)(batch->groups.size() + batch->passes.size());
 }
 
 int cfft_plan_launches(cfft_plan plan) {

@@ -96,6 +96,28 @@ int64_t cfft_plan_workspace_bytes(cfft_plan plan);
 /* Number of kernel launches one cfft_execute of this plan issues. */
 int cfft_plan_launches(cfft_plan plan);
 
+/* Batched form: `count` transforms of mixed lengths packed back to back in
+ * the order given (transform i starts at element sum(lengths[:i])).  The
+ * reference transforms one vector per call (fft_kernel!, src/kernel.jl:95-100,
+ * with one cached function per length); this plans every distinct length
+ * once and runs the whole batch as one CUDA graph: single-kernel transforms
+ * grouped into a few descriptor-driven launches, largest first, the rest on
+ * a shared scratch.  flags: CFFT_EXACT_TWIDDLES only. */
+typedef struct cfft_batch_s* cfft_batch;
+int cfft_batch_create(cfft_batch* batch, int64_t count, const int64_t* lengths, int dtype, int flags);
+
+/* Runs the batch (device pointers, in == out allowed) on `stream` as one
+ * graph launch; the graph is captured on the first call for a given
+ * (d_in, d_out, direction) and replayed after that. */
+int cfft_batch_execute(cfft_batch batch, const void* d_in, void* d_out, int direction, void* stream);
+
+/* Releases the batch, its plans, descriptors, scratch and graph. */
+int cfft_batch_destroy(cfft_batch batch);
+
+/* Total elements of the packed batch; kernel launches in its graph. */
+int64_t cfft_batch_elements(cfft_batch batch);
+int cfft_batch_launches(cfft_batch batch);
+
 /* No counterpart in the reference.  The two-pass FFT for callers that cannot
  * allocate device memory (an allocator-owned or capture-time context): the
  * scratch and twiddle tables live in one fixed __device__ array (32 MiB +

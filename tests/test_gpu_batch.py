@@ -1,0 +1,90 @@
+"""GPU tests of the batched form: one graph launch over mixed lengths.
+
+Every transform of a seeded mixed batch (half 7-smooth lengths, half with a
+prime factor up to 65537) must match the single-plan result of the same
+length: 1e-12 relative L2 for ComplexF64, and 1e-5 against the FP64 oracle
+for ComplexF32.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from _pkg import load
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def cb():
+    import torch
+    assert torch.cuda.is_available()
+    return load()
+
+
+def _lengths(cb, count, seed, hi):
+    import importlib
+    w = importlib.import_module("catabra_b200.workloads")
+    return w.batch_lengths(count, seed=seed, lo=16, hi=hi)
+
+
+@pytest.mark.parametrize("dtype,count,hi", [(np.complex128, 60, 1 << 17), (np.complex64, 80, 1 << 18)])
+def test_batch_matches_single_plans(cb, dtype, count, hi):
+    import torch
+    lengths = _lengths(cb, count, seed=count, hi=hi)
+    b = cb.Batch(lengths, dtype)
+    rng = np.random.default_rng(1)
+    x = (rng.standard_normal(b.total) + 1j * rng.standard_normal(b.total)).astype(dtype)
+    xd = torch.from_numpy(x).cuda()
+    y = b.execute(xd).cpu().numpy()
+    y2 = b.execute(xd).cpu().numpy()              # graph replay
+    assert np.array_equal(y, y2)
+    tol = 1e-12 if dtype == np.complex128 else 1e-5
+    for i, (o, n) in enumerate(zip(b.offsets, lengths)):
+        seg = x[o:o + n]
+        if dtype == np.complex128:
+            ref = cb.fft(seg)
+            assert rel(y[o:o + n], ref) < tol, (i, n)
+        elif i % 4 == 0:                           # FP32 form vs the FP64 oracle
+            ref = oracle.fft(seg.astype(np.complex128))
+            assert rel(y[o:o + n], ref) < tol, (i, n)
+    assert b.launches() >= 1
+    b.close()
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_batch_two_pass_members(cb, dtype):
+    """Lengths beyond one cluster run as grouped column/row passes over a
+    shared scratch; mixed with single-kernel lengths in the same batch."""
+    import torch
+    lengths = [16, 1 << 20, 531441, 4096, 999983, 30240, 65537, 300007, 1 << 19, 10007, 3]
+    b = cb.Batch(lengths, dtype)
+    rng = np.random.default_rng(5)
+    x = (rng.standard_normal(b.total) + 1j * rng.standard_normal(b.total)).astype(dtype)
+    y = b.execute(torch.from_numpy(x).cuda()).cpu().numpy()
+    tol = 1e-12 if dtype == np.complex128 else 1e-5
+    for o, n in zip(b.offsets, lengths):
+        seg = x[o:o + n]
+        ref = cb.fft(seg) if dtype == np.complex128 else oracle.fft(seg.astype(np.complex128))
+        assert rel(y[o:o + n], ref) < tol, n
+    b.close()
+
+
+def test_batch_inverse_roundtrip_inplace(cb):
+    import torch
+    lengths = _lengths(cb, 40, seed=7, hi=1 << 16)
+    b = cb.Batch(lengths, np.complex128)
+    rng = np.random.default_rng(2)
+    x = torch.from_numpy(rng.standard_normal(b.total) + 1j * rng.standard_normal(b.total)).cuda()
+    y = b.execute(x)
+    z = b.execute(y, cb.INVERSE, out=y)            # in place
+    assert (torch.linalg.norm(z - x) / torch.linalg.norm(x)).item() < 1e-12
+    b.close()
+
+
+def test_batch_rejects_bad_lengths(cb):
+    with pytest.raises(cb.CatabraError):
+        cb.Batch([16, 0, 32], np.complex64)
