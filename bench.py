@@ -191,7 +191,7 @@ def measure_e2e(torch, cb, lib, plans, bufs, args, world, dev):
     for (x, _, _), (n, b) in zip(bufs, SIZES):
         hin = torch.empty((b, n), dtype=torch.complex128, pin_memory=True)
         hin.copy_(x.cpu())
-        host.append((hin, torch.empty_like(hin)))
+        host.append((hin, torch.empty((b, n), dtype=torch.complex128, pin_memory=True)))
     torch.cuda.synchronize()
     vp = ctypes.c_void_p
     for h, (hin, hout) in zip(plans, host):          # warm the staging buffers
@@ -215,16 +215,315 @@ def measure_e2e(torch, cb, lib, plans, bufs, args, world, dev):
             "path": "cfft_execute_host (C ABI), pinned host buffers, fwd+inv of each batch"}
 
 
+# ---------------------------------------------------------------- other forms
+FORMS = ("plain", "small", "precision", "batch", "serve")
+
+
+def _setup_single():
+    import torch
+    rank, world, local = dist_env()
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _pkg import load
+    cb = load()
+    return torch, cb, cb._lib.LIB, torch.device("cuda", local)
+
+
+def _pct(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(round(q * (len(v) - 1))))]
+
+
+def form_small(torch, cb, lib, dev, args):
+    """1 x n=4096 ComplexF64: latency of one forward call."""
+    n = 4096
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    x = torch.complex(torch.randn(1, n, dtype=torch.float64, device=dev, generator=g),
+                      torch.randn(1, n, dtype=torch.float64, device=dev, generator=g))
+    y, z = torch.empty_like(x), torch.empty_like(x)
+    h = ctypes.c_void_p()
+    cb.check(lib.cfft_plan_create(ctypes.byref(h), n, 1, cb.C128, cb.NO_FLAG))
+    st = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(st.cuda_stream)
+    vp = ctypes.c_void_p
+    steps = max(args.steps, 200)
+    for _ in range(args.warmup + 10):
+        lib.cfft_execute(h, vp(x.data_ptr()), vp(y.data_ptr()), 0, sp)
+        lib.cfft_execute(h, vp(y.data_ptr()), vp(z.data_ptr()), 1, sp)
+    torch.cuda.synchronize()
+    err = (torch.linalg.norm(z - x) / torch.linalg.norm(x)).item()
+    dev_us, host_us = [], []
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        a.record(st)
+        lib.cfft_execute(h, vp(x.data_ptr()), vp(y.data_ptr()), 0, sp)
+        b.record(st)
+        b.synchronize()
+        host_us.append((time.perf_counter() - t0) * 1e6)
+        dev_us.append(a.elapsed_time(b) * 1e3)
+    # through the host entry: pinned 64 KiB in and out
+    hin = torch.empty((1, n), dtype=torch.complex128, pin_memory=True)
+    hin.copy_(x.cpu())
+    hout = torch.empty((1, n), dtype=torch.complex128, pin_memory=True)
+    e2e = []
+    for i in range(steps + 10):
+        t0 = time.perf_counter()
+        cb.check(lib.cfft_execute_host(h, vp(hin.data_ptr()), vp(hout.data_ptr()), 0))
+        if i >= 10:
+            e2e.append((time.perf_counter() - t0) * 1e6)
+    lib.cfft_plan_destroy(h)
+    return {"form": "small", "metric": "latency of one 4096-point ComplexF64 forward FFT",
+            "value": round(statistics.median(dev_us), 2), "unit": "us", "higher_is_better": False,
+            "p50_us": round(_pct(dev_us, 0.5), 2), "p99_us": round(_pct(dev_us, 0.99), 2),
+            "host_call_us_p50": round(_pct(host_us, 0.5), 2),
+            "e2e": {"value": round(statistics.median(e2e), 2), "unit": "us",
+                    "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n,
+                    "path": "cfft_execute_host, pinned host buffers"},
+            "roundtrip_rel_l2": err, "steps": steps, "dtype": "f64",
+            "config": {"workload": "1 x n=4096 C128, iid N(0,1)"}}
+
+
+def form_precision(torch, cb, lib, dev, args):
+    """ComplexF32 arithmetic with FP64-generated twiddles: 4096 x 2^16 and
+    4096 x 3^9, uniform(-1,1) parts; error vs this library's ComplexF64 path
+    (itself held to 1e-12 of the oracle by the tests)."""
+    sizes = [(65536, 4096), (19683, 4096)]
+    g = torch.Generator(device=dev)
+    g.manual_seed(11)
+    st = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(st.cuda_stream)
+    vp = ctypes.c_void_p
+    out = {}
+    total_bytes, total_ms = 0, 0.0
+    for n, b in sizes:
+        x = torch.complex(torch.rand(b, n, device=dev, generator=g) * 2 - 1,
+                          torch.rand(b, n, device=dev, generator=g) * 2 - 1)
+        y, z = torch.empty_like(x), torch.empty_like(x)
+        h = ctypes.c_void_p()
+        cb.check(lib.cfft_plan_create(ctypes.byref(h), n, b, cb.C64, cb.NO_FLAG))
+        for _ in range(args.warmup):
+            lib.cfft_execute(h, vp(x.data_ptr()), vp(y.data_ptr()), 0, sp)
+            lib.cfft_execute(h, vp(y.data_ptr()), vp(z.data_ptr()), 1, sp)
+        steps = max(3, min(args.steps, 50))
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(steps):
+            lib.cfft_execute(h, vp(x.data_ptr()), vp(y.data_ptr()), 0, sp)
+            lib.cfft_execute(h, vp(y.data_ptr()), vp(z.data_ptr()), 1, sp)
+        e.record(st)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(e) / (2 * steps)
+        rows = 64
+        xd = x[:rows].to(torch.complex128)
+        yd = torch.empty_like(xd)
+        h2 = ctypes.c_void_p()
+        cb.check(lib.cfft_plan_create(ctypes.byref(h2), n, rows, cb.C128, cb.NO_FLAG))
+        lib.cfft_execute(h2, vp(xd.data_ptr()), vp(yd.data_ptr()), 0, sp)
+        torch.cuda.synchronize()
+        rel = (torch.linalg.norm(y[:rows].to(torch.complex128) - yd) / torch.linalg.norm(yd)).item()
+        rt = (torch.linalg.norm(z - x) / torch.linalg.norm(x)).item()
+        desc = ctypes.create_string_buffer(256)
+        lib.cfft_plan_describe(h, desc, 256)
+        lib.cfft_plan_destroy(h)
+        lib.cfft_plan_destroy(h2)
+        nbytes = 2 * n * b * 8
+        out[str(n)] = {"ms_per_launch": round(ms, 4), "GB_s": round(nbytes / (ms * 1e-3) / 1e9, 2),
+                       "rel_l2_vs_f64": rel, "roundtrip_rel_l2": rt, "plan": desc.value.decode()}
+        total_bytes += nbytes
+        total_ms += ms
+        del x, y, z
+        torch.cuda.empty_cache()
+    peak, kind = load_peaks()
+    v = total_bytes / (total_ms * 1e-3) / 1e9
+    return {"form": "precision", "metric": "FFT GB/s, ComplexF32 with FP64 twiddles",
+            "value": round(v, 2), "unit": "GB/s", "higher_is_better": True, "per_size": out,
+            "frac_of_hbm": round(v / peak, 4), "peak": peak, "peak_kind": kind, "dtype": "f32",
+            "tolerance": 1e-5,
+            "config": {"workload": "C64 4096 x 2^16 and 4096 x 3^9, uniform(-1,1), forward"}}
+
+
+def form_batch(torch, cb, lib, dev, args):
+    """20000 mixed lengths in [16, 2^20] (half 7-smooth, half with a prime
+    factor <= 65537), one graph launch per execution; against the same
+    transforms as per-request plan executions."""
+    import importlib
+    w = importlib.import_module("catabra_b200.workloads")
+    lengths = [int(v) for v in w.batch_lengths(args.count, seed=1)]
+    vp = ctypes.c_void_p
+    st = torch.cuda.current_stream(dev)
+    sp = vp(st.cuda_stream)
+    res = {}
+    for name, dt, tdt, e in (("c64", np.complex64, torch.complex64, 8),
+                             ("c128", np.complex128, torch.complex128, 16)):
+        t0 = time.perf_counter()
+        b = cb.Batch(lengths, dt)
+        t_plan = time.perf_counter() - t0
+        x = torch.randn(b.total, dtype=tdt, device=dev)
+        y = torch.empty_like(x)
+        for _ in range(args.warmup):
+            b.execute(x, out=y)
+        steps = max(3, min(args.steps, 10))
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(steps):
+            b.execute(x, out=y)
+        z.record(st)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(z) / steps
+        plans = {}
+        for n in set(lengths):
+            h = ctypes.c_void_p()
+            cb.check(lib.cfft_plan_create(ctypes.byref(h), n, 1, cb.C128 if e == 16 else cb.C64, 0))
+            plans[n] = h
+        xp, yp = x.data_ptr(), y.data_ptr()
+
+        def per_request():
+            for o, n in zip(b.offsets, lengths):
+                lib.cfft_execute(plans[n], vp(xp + int(o) * e), vp(yp + int(o) * e), 0, sp)
+        per_request()
+        torch.cuda.synchronize()
+        a.record(st)
+        per_request()
+        z.record(st)
+        torch.cuda.synchronize()
+        ms_req = a.elapsed_time(z)
+        for h in plans.values():
+            lib.cfft_plan_destroy(h)
+        nbytes = 2 * b.total * e
+        res[name] = {"ms_per_batch": round(ms, 3), "GB_s": round(nbytes / (ms * 1e-3) / 1e9, 2),
+                     "per_request_ms": round(ms_req, 3),
+                     "per_request_GB_s": round(nbytes / (ms_req * 1e-3) / 1e9, 2),
+                     "speedup_vs_per_request": round(ms_req / ms, 2), "launches": b.launches(),
+                     "plan_s": round(t_plan, 2), "elements": b.total}
+        b.close()
+        del x, y
+        torch.cuda.empty_cache()
+    return {"form": "batch", "metric": "FFT GB/s, one graph launch over mixed lengths",
+            "value": res["c64"]["GB_s"], "unit": "GB/s", "higher_is_better": True, "per_dtype": res,
+            "config": {"workload": f"{args.count} lengths log-uniform in [16, 2^20], half 7-smooth, "
+                                   "half with a prime factor <= 65537 (seed 1), forward"}}
+
+
+def form_serve(torch, cb, lib, dev, args):
+    """Poisson arrivals at 50k req/s, n log-uniform in [64, 2^22] (80 % 7-smooth,
+    20 % with a prime factor <= 65537), ComplexF32, admission cap 64 GB.
+    The batched server (continuous batching) against per-request launches;
+    latency = completion - submission, both on the host's steady clock."""
+    import importlib
+    w = importlib.import_module("catabra_b200.workloads")
+    rate = 50000.0
+    reqs = w.request_stream(args.count, rate, seed=1)
+    lengths = [int(n) for _, n in reqs]
+    e = 8
+    # inputs and outputs cycle through two 8 GiB regions (far beyond L2), so
+    # requests in flight together read and write distinct memory
+    ring = (8 << 30) // e
+    xin = torch.randn(ring, dtype=torch.complex64, device=dev)
+    yout = torch.empty(ring, dtype=torch.complex64, device=dev)
+    offs, cur = [], 0
+    for n in lengths:
+        if cur + n > ring:
+            cur = 0
+        offs.append(cur)
+        cur += n
+    res = {}
+    for name, mode in (("batched", cb.SERVE_BATCHED), ("per_request", cb.SERVE_DIRECT)):
+        srv = cb.Server(np.complex64, mode=mode, max_inflight_bytes=64 << 30, max_requests=args.count + 256)
+        t0 = time.perf_counter()
+        distinct = sorted(set(lengths))
+        srv.prepare(distinct)
+        t_prep = time.perf_counter() - t0
+        for n in distinct[:: max(1, len(distinct) // 64)]:     # warm the kernel variants
+            srv.wait(srv.submit_ptr(n, xin.data_ptr(), yout.data_ptr()))
+        torch.cuda.synchronize()
+        base = srv.stats()
+        xp, yp = xin.data_ptr(), yout.data_ptr()
+        tickets = []
+        start = time.perf_counter()
+        for (ta, n), o in zip(reqs, offs):
+            while time.perf_counter() - start < ta:
+                pass
+            tickets.append(srv.submit_ptr(n, xp + o * e, yp + o * e))
+        t_sub_end = time.perf_counter() - start
+        srv.drain()
+        wall = time.perf_counter() - start
+        lat_ms = [srv.query(t) / 1e3 for t in tickets]
+        st = srv.stats()
+        srv.close()
+        nbytes = 2 * e * sum(lengths)
+        res[name] = {"p50_ms": round(_pct(lat_ms, 0.5), 3), "p99_ms": round(_pct(lat_ms, 0.99), 3),
+                     "mean_ms": round(statistics.mean(lat_ms), 3),
+                     "req_per_s": round(len(lengths) / wall, 1), "GB_s": round(nbytes / wall / 1e9, 2),
+                     "wall_s": round(wall, 3), "submit_s": round(t_sub_end, 3),
+                     "batches": st["batches"] - base["batches"],
+                     "launches": st["launches"] - base["launches"], "prepare_s": round(t_prep, 1)}
+    del xin, yout
+    torch.cuda.empty_cache()
+    b, d = res["batched"], res["per_request"]
+    return {"form": "serve", "metric": "p50/p99 latency and req/s under Poisson arrivals",
+            "value": b["p99_ms"], "unit": "ms (p99, batched)", "higher_is_better": False,
+            "modes": res, "speedup_req_per_s": round(b["req_per_s"] / d["req_per_s"], 2),
+            "dtype": "f32",
+            "config": {"workload": f"{args.count} requests, Poisson {rate:.0f} req/s (seed 1), n log-uniform "
+                                   "in [64, 2^22], 80% 7-smooth / 20% prime-containing, C64, forward, "
+                                   "admission cap 64 GiB, plans prepared before traffic"}}
+
+
+def run_form(args):
+    env = _setup_single()
+    if env is None:
+        return 0
+    torch, cb, lib, dev = env
+    fn = {"small": form_small, "precision": form_precision, "batch": form_batch,
+          "serve": form_serve}[args.form]
+    line = fn(torch, cb, lib, dev, args)
+    line.update({"n_gpus": 1, "warmup": args.warmup, "data": "synthetic (seeded)"})
+    print(json.dumps(line))
+    return 0
+
+
+def measure_library(torch, bufs, stream, steps=20):
+    """Run-only comparison: torch.fft (cuFFT) on the same resident batches,
+    fwd + inv per step.  Not the product; reported for context."""
+    per = {}
+    total = 0.0
+    for (x, y, z), (n, b) in zip(bufs, SIZES):
+        for _ in range(3):
+            torch.fft.ifft(torch.fft.fft(x, dim=1), dim=1)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(steps):
+            torch.fft.ifft(torch.fft.fft(x, dim=1), dim=1)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(e) / steps
+        per[str(n)] = round(ms / 2, 4)
+        total += ms
+    return {"value": round(algorithmic_bytes_per_step() / (total * 1e-3) / 1e9, 3), "unit": "GB/s",
+            "ms_per_step": round(total, 4), "ms_per_launch": per,
+            "impl": "torch.fft (cuFFT), same batches, fwd + inv"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--only", type=int, default=0, help="restrict to one transform length")
     ap.add_argument("--batch", type=int, default=0, help="override the batch (profiling cases)")
     ap.add_argument("--quick", action="store_true", help="skip the e2e and CPU-baseline legs")
+    ap.add_argument("--form", default="plain", choices=FORMS,
+                    help="plain (the contract line) or one of the other workload forms")
+    ap.add_argument("--count", type=int, default=20000, help="batch/serve form: transforms")
     args = ap.parse_args()
     global SIZES
     if args.only:
@@ -234,6 +533,8 @@ def main():
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(3, args.warmup)
+    if args.form != "plain":
+        return run_form(args)
 
     import torch
     rank, world, local = dist_env()
@@ -318,6 +619,7 @@ def main():
     traffic = load_traffic().get(f"four_c128_n{n_dom}_b{b_dom}")
 
     e2e = None if args.quick else measure_e2e(torch, cb, lib, plans, bufs, args, world, dev)
+    cufft = None if args.quick else measure_library(torch, bufs, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.quick:
@@ -346,6 +648,7 @@ def main():
                          "ms_per_launch": round(ms_launch, 4)},
             "per_size_ms_per_launch": {str(n): round(m, 4) for n, _, m, _ in per},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "library_comparison": cufft,
             "clocks": clk.summary(),
         }
         print(json.dumps(line))

@@ -29,12 +29,12 @@ import numpy as np
 
 from . import _lib
 from ._lib import (BACKWARD, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERSE, MEASURE,
-                   NO_FLAG, CatabraError, check)
+                   NO_FLAG, SERVE_BATCHED, SERVE_DIRECT, CatabraError, check)
 
 FLAG = int
 PLANNER_DEFAULT = NO_FLAG
 
-__all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache", "Batch",
+__all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache", "Batch", "Server",
            "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
            "describe_strategy", "version"]
 
@@ -285,6 +285,75 @@ class Batch:
     def close(self):
         if getattr(self, "handle", None):
             _lib.LIB.cfft_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving form: requests submitted one at a time, batched on the device.
+
+    ``Server(dtype, mode=SERVE_BATCHED, max_inflight_bytes=0)``;
+    ``t = s.submit(x, y, direction)`` queues the transform of the 1-D CUDA
+    tensor ``x`` into ``y`` (same length and type) and returns a ticket;
+    ``s.wait(t)`` blocks until it is done and returns its latency in
+    microseconds.  The tensors must stay alive until the request is done.
+    ``mode=SERVE_DIRECT`` launches each request on arrival instead (the
+    per-request path).
+    """
+
+    def __init__(self, dtype=np.complex64, mode: int = SERVE_BATCHED, max_inflight_bytes: int = 0,
+                 max_requests: int = 0):
+        h = ctypes.c_void_p()
+        self.dtype_code = _dtype_code(dtype)
+        check(_lib.LIB.cfft_serve_create(ctypes.byref(h), self.dtype_code, int(max_inflight_bytes),
+                                         int(max_requests), int(mode)))
+        self.handle = h
+
+    def prepare(self, lengths) -> None:
+        arr = (ctypes.c_int64 * len(lengths))(*[int(n) for n in lengths])
+        check(_lib.LIB.cfft_serve_prepare(self.handle, len(lengths), arr))
+
+    def submit(self, x, y, direction: int = FORWARD) -> int:
+        if not (_is_torch(x) and x.is_cuda and x.is_contiguous() and y.is_contiguous()
+                and x.numel() == y.numel()):
+            raise ValueError("expected contiguous CUDA tensors of equal length")
+        if _dtype_code(x.dtype) != self.dtype_code or _dtype_code(y.dtype) != self.dtype_code:
+            raise TypeError("element type does not match the server")
+        return self.submit_ptr(x.numel(), x.data_ptr(), y.data_ptr(), direction)
+
+    def submit_ptr(self, n: int, d_in: int, d_out: int, direction: int = FORWARD) -> int:
+        t = ctypes.c_int64()
+        check(_lib.LIB.cfft_serve_submit(self.handle, int(n), ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                         int(direction), ctypes.byref(t)))
+        return t.value
+
+    def query(self, ticket: int):
+        """Latency in microseconds once done, else None."""
+        done, lat = ctypes.c_int(), ctypes.c_double()
+        check(_lib.LIB.cfft_serve_query(self.handle, int(ticket), ctypes.byref(done), ctypes.byref(lat)))
+        return lat.value if done.value else None
+
+    def wait(self, ticket: int) -> float:
+        lat = ctypes.c_double()
+        check(_lib.LIB.cfft_serve_wait(self.handle, int(ticket), ctypes.byref(lat)))
+        return lat.value
+
+    def drain(self) -> None:
+        check(_lib.LIB.cfft_serve_drain(self.handle))
+
+    def stats(self):
+        r, b, l = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(_lib.LIB.cfft_serve_stats(self.handle, ctypes.byref(r), ctypes.byref(b), ctypes.byref(l)))
+        return {"requests": r.value, "batches": b.value, "launches": l.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            check(_lib.LIB.cfft_serve_destroy(self.handle))
             self.handle = None
 
     def __del__(self):

@@ -15,6 +15,7 @@ C128, C64 = 0, 1
 FORWARD, INVERSE, BACKWARD = 0, 1, 2
 NO_FLAG, MEASURE, ENCHANT, EXACT_TWIDDLES = 0, 1, 2, 16
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED = 0, 1, 2, 3, 4
+SERVE_BATCHED, SERVE_DIRECT = 0, 1
 
 # every symbol include/catabra_b200.h declares, with (restype, argtypes)
 _i64, _vp, _ci, _cp = ctypes.c_int64, ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p
@@ -37,6 +38,14 @@ SIGNATURES = {
     "cfft_batch_destroy": (_ci, [_vp]),
     "cfft_batch_elements": (_i64, [_vp]),
     "cfft_batch_launches": (_ci, [_vp]),
+    "cfft_serve_create": (_ci, [ctypes.POINTER(_vp), _ci, _i64, _i64, _ci]),
+    "cfft_serve_prepare": (_ci, [_vp, _i64, ctypes.POINTER(_i64)]),
+    "cfft_serve_submit": (_ci, [_vp, _i64, _vp, _vp, _ci, ctypes.POINTER(_i64)]),
+    "cfft_serve_query": (_ci, [_vp, _i64, ctypes.POINTER(_ci), ctypes.POINTER(ctypes.c_double)]),
+    "cfft_serve_wait": (_ci, [_vp, _i64, ctypes.POINTER(ctypes.c_double)]),
+    "cfft_serve_drain": (_ci, [_vp]),
+    "cfft_serve_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "cfft_serve_destroy": (_ci, [_vp]),
 }
 
 

@@ -75,7 +75,7 @@ struct BatchLaunch {
     const int* block_desc;
     const void* in_base;
     void* out_base;
-    int dir;
+    int dir;                      // direction of every block, or -1: each block's own
     int pad_;
 };
 

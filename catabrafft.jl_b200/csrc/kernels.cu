@@ -38,8 +38,10 @@ __device__ __forceinline__ const KParams& stage_params(const BatchLaunch& L, KPa
         KParams p = L.desc[L.block_desc[blockIdx.x]];
         if (p.in_user) p.in = (const V*)L.in_base + p.in_off;
         if (p.out_user) p.out = (V*)L.out_base + p.out_off;
-        p.dir = L.dir;
-        if (L.dir != 1) p.scale = 1.0;
+        if (L.dir >= 0) {                 // one direction for the launch
+            p.dir = L.dir;
+            if (L.dir != 1) p.scale = 1.0;
+        }                                 // else: per-block direction and scale
         *sp = p;
     }
     __syncthreads();

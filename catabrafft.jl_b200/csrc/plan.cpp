@@ -14,7 +14,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -421,10 +426,17 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
         int c2 = conv;
         int64_t M2 = M;
         if (conv == CONV_RADER) { c2 = CONV_BLUE; M2 = smooth_ceil(2 * n - 1); }
+        // a convolution may use any 7-smooth length >= its minimum: take the
+        // first that splits into two factors of at most 4096
         Shape g;
-        if (global_shape(M2, dtype, g)) {
-            g.conv = c2;
-            v.push_back(g);
+        for (int tries = 0; tries < 256; tries++) {
+            if (global_shape(M2, dtype, g)) {
+                g.conv = c2;
+                v.push_back(g);
+                break;
+            }
+            if (c2 == CONV_NONE) break;
+            M2 = smooth_ceil(M2 + 1);
         }
     }
     return v;
@@ -1053,6 +1065,53 @@ static void batch_free(cfft_batch_s* B) {
     B->allocs.clear();
 }
 
+// a batch-1 plan whose two-pass scratch is supplied by its caller (batched
+// and serving forms)
+static int build_shared_plan(int64_t n, int dtype, int flags, int device, cfft_plan_s** out) {
+    if (n > (1LL << 26)) return fail(CFFT_ERR_UNSUPPORTED, "length above 2^26");
+    auto cands = candidate_shapes(n, dtype, 1);
+    cfft_plan_s* P = new cfft_plan_s();
+    P->n = n;
+    P->batch = 1;
+    P->dtype = dtype;
+    P->flags = flags;
+    P->device = device;
+    P->shared_scratch = true;
+    int rc = fail(CFFT_ERR_UNSUPPORTED, "no execution shape for n=" + std::to_string(n));
+    for (auto& c : cands) {
+        rc = plan_build(P, c);
+        if (rc == CFFT_OK) break;
+        plan_free(P);
+    }
+    if (rc) {
+        delete P;
+        return rc;
+    }
+    *out = P;
+    return CFFT_OK;
+}
+static bool single_kernel(const cfft_plan_s* P) {
+    return P->stages.size() == 1 &&
+           (P->stages[0].kp.mode == MODE_ROWS || P->stages[0].kp.mode == MODE_FOUR);
+}
+// CTAs one parameter block occupies in a batched launch
+static int blocks_for(const KParams& kp) {
+    if (kp.mode == MODE_FOUR) return kp.C;
+    if (kp.mode == MODE_COLPASS) return kp.N2 / kp.V;
+    if (kp.mode == MODE_ROWPASS) return kp.N1 / kp.V;
+    return 1;
+}
+// single-kernel stage -> its batched kernel variant (and the parameter fix-up
+// that variant needs)
+static const void* batched_variant(KParams& kp, int dtype) {
+    int kmode = kp.mode;
+    if (kp.mode == MODE_FOUR) {
+        if (kp.pa.Gwarp > 0 && kp.pc.Gwarp > 0) kmode = MODE_FOUR_WARP;
+        else kp.pa.Gwarp = kp.pc.Gwarp = 0;
+    }
+    return cfft_batch_kernel_for(kmode, dtype);
+}
+
 // launches are grouped by how many CTAs fit an SM (two below ~113 KB of
 // shared memory, one above); a group runs with its largest member's size
 static int smem_class(size_t smem) { return smem <= (size_t)112 * 1024 ? 0 : 1; }
@@ -1070,10 +1129,7 @@ static int make_group(cfft_batch_s* B, const void* fn, int cluster, std::vector<
     for (auto& it : items) {
         KParams kp = it.kp;
         kp.blk0 = (int)map.size();
-        int nb = 1;
-        if (kp.mode == MODE_FOUR) nb = kp.C;
-        else if (kp.mode == MODE_COLPASS) nb = kp.N2 / kp.V;
-        else if (kp.mode == MODE_ROWPASS) nb = kp.N1 / kp.V;
+        const int nb = blocks_for(kp);
         for (int b = 0; b < nb; b++) map.push_back((int)desc.size());
         desc.push_back(kp);
         g.cost += it.cost;
@@ -1111,25 +1167,9 @@ static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* leng
     // one plan per distinct length (batch 1, scratch shared by the batch)
     for (int64_t n : B->len) {
         if (B->plans.count(n)) continue;
-        if (n > (1LL << 26)) return fail(CFFT_ERR_UNSUPPORTED, "length above 2^26");
-        auto cands = candidate_shapes(n, dtype, 1);
-        cfft_plan_s* P = new cfft_plan_s();
-        P->n = n;
-        P->batch = 1;
-        P->dtype = dtype;
-        P->flags = B->flags;
-        P->device = B->device;
-        P->shared_scratch = true;
-        int rc = CFFT_ERR_UNSUPPORTED;
-        for (auto& c : cands) {
-            rc = plan_build(P, c);
-            if (rc == CFFT_OK) break;
-            plan_free(P);
-        }
-        if (rc) {
-            delete P;
-            return rc;
-        }
+        cfft_plan_s* P = nullptr;
+        int rc = build_shared_plan(n, dtype, B->flags, B->device, &P);
+        if (rc) return rc;
         B->plans[n] = P;
     }
     // group single-kernel transforms; collect the two-pass ones
@@ -1139,19 +1179,14 @@ static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* leng
     for (int64_t i = 0; i < count; i++) {
         cfft_plan_s* P = B->plans[B->len[i]];
         const double cost = (double)P->shape.M * std::log2((double)std::max<int64_t>(2, P->shape.M));
-        if (P->stages.size() == 1 && (P->stages[0].kp.mode == MODE_ROWS || P->stages[0].kp.mode == MODE_FOUR)) {
+        if (single_kernel(P)) {
             KParams kp = P->stages[0].kp;
-            int kmode = kp.mode;
-            if (kp.mode == MODE_FOUR) {
-                if (kp.pa.Gwarp > 0 && kp.pc.Gwarp > 0) kmode = MODE_FOUR_WARP;
-                else kp.pa.Gwarp = kp.pc.Gwarp = 0;
-            }
+            const void* fn = batched_variant(kp, dtype);
             kp.batch = 1;
             kp.in_off = kp.out_off = B->off[i];
             kp.in_user = kp.out_user = 1;
             kp.in_dist = kp.out_dist = B->len[i];
             kp.scale = 1.0 / (double)B->len[i];
-            const void* fn = cfft_batch_kernel_for(kmode, dtype);
             bins[std::make_tuple(fn, P->stages[0].cluster, smem_class(P->stages[0].smem))]
                 .push_back({i, kp, cost, P->stages[0].smem});
         } else {
@@ -1269,6 +1304,395 @@ static int batch_enqueue(cfft_batch_s* B, const void* in, void* out, int dir, cu
         }
     }
     B->launches = launches;
+    return CFFT_OK;
+}
+
+// ------------------------------------------------------------ serving form
+// Requests (n, device input, device output, direction) arrive one at a time
+// from any host thread.  Batched mode: a worker thread forms a micro-batch
+// from everything queued whenever one of its launch slots is idle
+// (continuous batching: the next batch forms while earlier ones run),
+// admitting requests in arrival order while the bytes in flight (input +
+// output + two-pass scratch) stay under the cap, and runs the batch as
+// grouped descriptor launches on the slot's stream, each request's
+// direction in its own parameter block.  Direct mode: every request is
+// launched on arrival through its own cached plan (the per-request
+// baseline).  The worker observes completion by polling events; a request's
+// latency is its completion time minus its submission time on the host's
+// steady clock.
+static double now_us() {
+    return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct ServeReq {
+    int64_t n = 0;
+    const void* in = nullptr;
+    void* out = nullptr;
+    int dir = 0;
+    double t_sub = 0, t_done = 0;
+    std::atomic<int> state{0};    // 0 queued, 1 launched, 2 done, < 0 failed (-status)
+};
+
+struct ServeSlot {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    char* h_desc = nullptr;       // pinned staging of parameter blocks and block maps
+    char* d_desc = nullptr;
+    size_t desc_cap = 0;
+    void* scratch = nullptr;
+    size_t scratch_cap = 0;
+    std::vector<int64_t> reqs;
+    size_t bytes = 0;
+    bool busy = false;
+};
+
+struct cfft_server_s {
+    int dtype = 0, device = 0, mode = 0;
+    size_t cap = 0;
+    int64_t capacity = 0;
+    std::unique_ptr<ServeReq[]> req;
+    std::atomic<int64_t> next{0};
+    std::mutex qmu;                           // queue, direct-mode launches
+    std::condition_variable qcv;
+    std::deque<int64_t> queue;
+    std::deque<std::pair<int64_t, cudaEvent_t>> dpending;
+    std::vector<cudaEvent_t> evpool;
+    std::mutex dmu;                           // completion notification
+    std::condition_variable dcv;
+    std::mutex pmu;                           // plan caches
+    std::map<int64_t, cfft_plan_s*> plans;    // caller-scratch plans (batched mode)
+    std::map<int64_t, cfft_plan_s*> dplans;   // direct-mode plans (scratch: dscratch)
+    void* dscratch = nullptr;                 // direct mode: one stream, one scratch
+    size_t dscratch_cap = 0;
+    std::vector<ServeSlot> slots;
+    size_t inflight = 0;                      // worker only
+    std::atomic<bool> stop{false};
+    std::thread worker;
+    cudaStream_t dstream = nullptr;
+    std::atomic<int64_t> batches{0}, launches{0}, done{0};
+    std::mutex emu;
+    std::string errmsg;
+};
+
+static const size_t kServeAlign = 256;
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+static int serve_plan(cfft_server_s* S, int64_t n, bool direct, cfft_plan_s** out) {
+    std::lock_guard<std::mutex> lk(S->pmu);
+    auto& m = direct ? S->dplans : S->plans;
+    auto it = m.find(n);
+    if (it != m.end()) {
+        *out = it->second;
+        return CFFT_OK;
+    }
+    cfft_plan_s* P = nullptr;
+    int rc = build_shared_plan(n, S->dtype, 0, S->device, &P);
+    if (rc) return rc;
+    m[n] = P;
+    *out = P;
+    return CFFT_OK;
+}
+static size_t serve_scratch(const cfft_plan_s* P) {
+    if (single_kernel(P)) return 0;
+    const size_t one = align_up((size_t)P->shape.M * elem_bytes(P->dtype), kServeAlign);
+    return P->stages.size() > 2 ? 2 * one : one;
+}
+static void serve_error(cfft_server_s* S, const std::string& msg) {
+    std::lock_guard<std::mutex> lk(S->emu);
+    S->errmsg = msg;
+}
+static void serve_finish(cfft_server_s* S, const std::vector<int64_t>& reqs, int state) {
+    const double t = now_us();
+    {
+        std::lock_guard<std::mutex> lk(S->dmu);
+        for (int64_t r : reqs) {
+            S->req[r].t_done = t;
+            S->req[r].state.store(state);
+        }
+    }
+    S->done += (int64_t)reqs.size();
+    S->dcv.notify_all();
+}
+
+// one micro-batch on an idle slot: grouped launches, then the slot's event
+static int serve_launch(cfft_server_s* S, ServeSlot& sl) {
+    struct It { KParams kp; double cost; size_t smem; };
+    std::map<std::tuple<const void*, int, int>, std::vector<It>> singles;
+    std::map<std::tuple<const void*, int>, std::vector<It>> pass[4];
+    size_t scur = 0;
+    for (int64_t t : sl.reqs) {
+        ServeReq& r = S->req[t];
+        cfft_plan_s* P = nullptr;
+        int rc = serve_plan(S, r.n, false, &P);
+        if (rc) return rc;
+        const double scale = (r.dir == CFFT_INVERSE) ? 1.0 / (double)r.n : 1.0;
+        const double cost = (double)P->shape.M;
+        if (single_kernel(P)) {
+            KParams kp = P->stages[0].kp;
+            const void* fn = batched_variant(kp, S->dtype);
+            kp.batch = 1;
+            kp.in = r.in;
+            kp.out = r.out;
+            kp.in_user = kp.out_user = 0;
+            kp.in_off = kp.out_off = 0;
+            kp.in_dist = kp.out_dist = r.n;
+            kp.dir = r.dir;
+            kp.scale = scale;
+            singles[std::make_tuple(fn, P->stages[0].cluster, smem_class(P->stages[0].smem))]
+                .push_back({kp, cost, P->stages[0].smem});
+            continue;
+        }
+        const size_t one = align_up((size_t)P->shape.M * elem_bytes(S->dtype), kServeAlign);
+        char* s1 = (char*)sl.scratch + scur;
+        char* s2 = s1 + one;
+        scur += serve_scratch(P);
+        for (size_t k = 0; k < P->stages.size() && k < 4; k++) {
+            const Stage& st = P->stages[k];
+            KParams kp = st.kp;
+            auto where = [&](int sel) -> void* {
+                return sel == 0 ? (void*)r.in : sel == 1 ? r.out : sel == 2 ? (void*)s1 : (void*)s2;
+            };
+            kp.batch = 1;
+            kp.in = where(st.in_sel);
+            kp.out = where(st.out_sel);
+            kp.in_dist = (st.in_sel >= 2) ? P->shape.M : r.n;
+            kp.out_dist = (st.out_sel >= 2) ? P->shape.M : r.n;
+            kp.in_user = kp.out_user = 0;
+            kp.in_off = kp.out_off = 0;
+            kp.dir = r.dir;
+            kp.scale = scale;
+            pass[k][std::make_tuple(cfft_batch_kernel_for(kp.mode, S->dtype), smem_class(st.smem))]
+                .push_back({kp, cost, st.smem});
+        }
+    }
+    // pack every group's parameter blocks and block map into one upload
+    struct G { const void* fn; int cluster; size_t smem; size_t doff, moff; unsigned grid; };
+    std::vector<G> gs;
+    std::vector<char> host;
+    auto add = [&](const void* fn, int cluster, std::vector<It>& items) {
+        std::stable_sort(items.begin(), items.end(), [](const It& a, const It& b) { return a.cost > b.cost; });
+        G g{fn, cluster, 0, 0, 0, 0};
+        std::vector<int> map;
+        std::vector<KParams> desc;
+        for (auto& it : items) {
+            KParams kp = it.kp;
+            kp.blk0 = (int)map.size();
+            for (int b = 0; b < blocks_for(kp); b++) map.push_back((int)desc.size());
+            desc.push_back(kp);
+            g.smem = std::max(g.smem, it.smem);
+        }
+        g.grid = (unsigned)map.size();
+        g.doff = align_up(host.size(), 16);
+        host.resize(g.doff + desc.size() * sizeof(KParams));
+        memcpy(host.data() + g.doff, desc.data(), desc.size() * sizeof(KParams));
+        g.moff = align_up(host.size(), 16);
+        host.resize(g.moff + map.size() * sizeof(int));
+        memcpy(host.data() + g.moff, map.data(), map.size() * sizeof(int));
+        gs.push_back(g);
+    };
+    for (auto& kv : singles) add(std::get<0>(kv.first), std::get<1>(kv.first), kv.second);
+    std::stable_sort(gs.begin(), gs.end(), [](const G& a, const G& b) { return a.grid > b.grid; });
+    for (int k = 0; k < 4; k++)
+        for (auto& kv : pass[k]) add(std::get<0>(kv.first), 1, kv.second);
+    if (host.size() > sl.desc_cap) {
+        if (sl.h_desc) cudaFreeHost(sl.h_desc);
+        if (sl.d_desc) cudaFree(sl.d_desc);
+        sl.h_desc = sl.d_desc = nullptr;
+        sl.desc_cap = 0;
+        const size_t capb = align_up(host.size() * 2, 1 << 16);
+        CUDA_TRY(cudaHostAlloc((void**)&sl.h_desc, capb, cudaHostAllocDefault));
+        CUDA_TRY(cudaMalloc((void**)&sl.d_desc, capb));
+        sl.desc_cap = capb;
+    }
+    memcpy(sl.h_desc, host.data(), host.size());
+    CUDA_TRY(cudaMemcpyAsync(sl.d_desc, sl.h_desc, host.size(), cudaMemcpyHostToDevice, sl.st));
+    for (auto& g : gs) {
+        CUDA_TRY(cfft_prepare_fn(g.fn, g.smem, g.cluster));
+        BatchLaunch L;
+        L.desc = (const KParams*)(sl.d_desc + g.doff);
+        L.block_desc = (const int*)(sl.d_desc + g.moff);
+        L.in_base = nullptr;
+        L.out_base = nullptr;
+        L.dir = -1;
+        L.pad_ = 0;
+        cudaError_t ce = cfft_launch_batch(g.fn, L, g.grid, g.smem, g.cluster, sl.st);
+        if (ce != cudaSuccess) return fail(CFFT_ERR_CUDA, std::string("serve launch: ") + cudaGetErrorString(ce));
+    }
+    CUDA_TRY(cudaEventRecord(sl.ev, sl.st));
+    S->batches++;
+    S->launches += (int64_t)gs.size();
+    return CFFT_OK;
+}
+
+static void serve_worker(cfft_server_s* S) {
+    cudaSetDevice(S->device);
+    const size_t e = elem_bytes(S->dtype);
+    std::vector<int64_t> done;
+    while (true) {
+        bool progressed = false;
+        bool busy = false;
+        for (auto& sl : S->slots) {
+            if (!sl.busy) continue;
+            const cudaError_t q = cudaEventQuery(sl.ev);
+            if (q == cudaErrorNotReady) { busy = true; continue; }
+            if (q != cudaSuccess) serve_error(S, std::string("serve batch: ") + cudaGetErrorString(q));
+            serve_finish(S, sl.reqs, q == cudaSuccess ? 2 : -CFFT_ERR_CUDA);
+            S->inflight -= sl.bytes;
+            sl.reqs.clear();
+            sl.bytes = 0;
+            sl.busy = false;
+            progressed = true;
+        }
+        if (S->mode == CFFT_SERVE_DIRECT) {   // completions in launch order
+            std::unique_lock<std::mutex> lk(S->qmu);
+            while (!S->dpending.empty()) {
+                const cudaError_t q = cudaEventQuery(S->dpending.front().second);
+                if (q == cudaErrorNotReady) { busy = true; break; }
+                done.assign(1, S->dpending.front().first);
+                S->evpool.push_back(S->dpending.front().second);
+                S->dpending.pop_front();
+                lk.unlock();
+                if (q != cudaSuccess) serve_error(S, std::string("serve request: ") + cudaGetErrorString(q));
+                serve_finish(S, done, q == cudaSuccess ? 2 : -CFFT_ERR_CUDA);
+                progressed = true;
+                lk.lock();
+            }
+        }
+        ServeSlot* idle = nullptr;
+        for (auto& sl : S->slots)
+            if (!sl.busy) { idle = &sl; break; }
+        if (S->mode == CFFT_SERVE_BATCHED && idle) {
+            // admit in arrival order under the cap (a request alone always runs)
+            size_t scr = 0;
+            for (;;) {
+                int64_t t;
+                {
+                    std::lock_guard<std::mutex> lk(S->qmu);
+                    if (S->queue.empty()) break;
+                    t = S->queue.front();
+                    S->queue.pop_front();
+                }
+                ServeReq& r = S->req[t];
+                cfft_plan_s* P = nullptr;
+                int rc = serve_plan(S, r.n, false, &P);
+                if (rc) {
+                    serve_error(S, cfft_last_error());
+                    serve_finish(S, std::vector<int64_t>(1, t), -rc);
+                    continue;
+                }
+                const size_t sneed = serve_scratch(P);
+                const size_t need = 2 * (size_t)r.n * e + sneed;
+                const bool alone = idle->reqs.empty() && S->inflight == 0;
+                if (!alone && (S->inflight + idle->bytes + need > S->cap || scr + sneed > idle->scratch_cap)) {
+                    std::lock_guard<std::mutex> lk(S->qmu);
+                    S->queue.push_front(t);
+                    break;
+                }
+                if (scr + sneed > idle->scratch_cap) {
+                    // grow (only when this request alone does not fit; the slot is idle)
+                    if (idle->scratch) cudaFree(idle->scratch);
+                    idle->scratch = nullptr;
+                    idle->scratch_cap = 0;
+                    if (cudaMalloc(&idle->scratch, scr + sneed) != cudaSuccess) {
+                        cudaGetLastError();
+                        serve_error(S, "serve: scratch allocation failed");
+                        serve_finish(S, std::vector<int64_t>(1, t), -CFFT_ERR_NOMEM);
+                        continue;
+                    }
+                    idle->scratch_cap = scr + sneed;
+                }
+                scr += sneed;
+                idle->reqs.push_back(t);
+                idle->bytes += need;
+                r.state.store(1);
+            }
+            if (!idle->reqs.empty()) {
+                int rc = serve_launch(S, *idle);
+                if (rc) {
+                    serve_error(S, cfft_last_error());
+                    cudaStreamSynchronize(idle->st);
+                    serve_finish(S, idle->reqs, -rc);
+                    idle->reqs.clear();
+                    idle->bytes = 0;
+                } else {
+                    S->inflight += idle->bytes;
+                    idle->busy = true;
+                    busy = true;
+                }
+                progressed = true;
+            }
+        }
+        if (progressed) continue;
+        bool queued;
+        {
+            std::lock_guard<std::mutex> lk(S->qmu);
+            queued = !S->queue.empty() || !S->dpending.empty();
+        }
+        if (S->stop.load() && !busy && !queued) break;
+        if (busy || queued) {
+            std::this_thread::yield();
+        } else {
+            std::unique_lock<std::mutex> lk(S->qmu);
+            S->qcv.wait_for(lk, std::chrono::milliseconds(2),
+                            [&] { return !S->queue.empty() || !S->dpending.empty() || S->stop.load(); });
+        }
+    }
+}
+
+static void serve_free(cfft_server_s* S) {
+    if (S->worker.joinable()) {
+        S->stop.store(true);
+        S->qcv.notify_all();
+        S->worker.join();
+    }
+    for (auto& sl : S->slots) {
+        if (sl.st) cudaStreamSynchronize(sl.st);
+        if (sl.st) cudaStreamDestroy(sl.st);
+        if (sl.ev) cudaEventDestroy(sl.ev);
+        if (sl.h_desc) cudaFreeHost(sl.h_desc);
+        if (sl.d_desc) cudaFree(sl.d_desc);
+        if (sl.scratch) cudaFree(sl.scratch);
+    }
+    S->slots.clear();
+    if (S->dstream) {
+        cudaStreamSynchronize(S->dstream);
+        cudaStreamDestroy(S->dstream);
+    }
+    if (S->dscratch) cudaFree(S->dscratch);
+    for (auto& pe : S->dpending) cudaEventDestroy(pe.second);
+    for (cudaEvent_t ev : S->evpool) cudaEventDestroy(ev);
+    for (auto* m : {&S->plans, &S->dplans})
+        for (auto& kv : *m) {
+            plan_free(kv.second);
+            delete kv.second;
+        }
+}
+
+static int serve_create_impl(cfft_server_s* S, int dtype, int64_t max_inflight_bytes, int64_t max_requests,
+                             int mode) {
+    if (dtype != CFFT_C128 && dtype != CFFT_C64) return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128 or CFFT_C64");
+    if (mode != CFFT_SERVE_BATCHED && mode != CFFT_SERVE_DIRECT)
+        return fail(CFFT_ERR_INVALID, "mode must be CFFT_SERVE_BATCHED or CFFT_SERVE_DIRECT");
+    if (max_inflight_bytes < 0 || max_requests < 0) return fail(CFFT_ERR_INVALID, "negative limit");
+    S->dtype = dtype;
+    S->mode = mode;
+    cudaGetDevice(&S->device);
+    S->cap = max_inflight_bytes ? (size_t)max_inflight_bytes : ((size_t)64 << 30);
+    S->capacity = max_requests ? max_requests : (1 << 18);
+    S->req.reset(new ServeReq[(size_t)S->capacity]);
+    if (mode == CFFT_SERVE_BATCHED) {
+        S->slots.resize(3);
+        for (auto& sl : S->slots) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
+            sl.scratch_cap = std::min<size_t>(S->cap / 4, (size_t)1 << 30);
+            CUDA_TRY(cudaMalloc(&sl.scratch, sl.scratch_cap));
+        }
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&S->dstream, cudaStreamNonBlocking));
+    }
+    S->worker = std::thread(serve_worker, S);
     return CFFT_OK;
 }
 
@@ -1479,3 +1903,157 @@ int cfft_plan_launches(cfft_plan plan) {
 }
 
 }  // extern "C"
+
+int cfft_serve_create(cfft_server* server, int dtype, int64_t max_inflight_bytes, int64_t max_requests,
+                      int mode) {
+    g_err[0] = 0;
+    if (!server) return fail(CFFT_ERR_INVALID, "server pointer is null");
+    *server = nullptr;
+    cfft_server_s* S = new cfft_server_s();
+    int rc = serve_create_impl(S, dtype, max_inflight_bytes, max_requests, mode);
+    if (rc) {
+        serve_free(S);
+        delete S;
+        return rc;
+    }
+    *server = S;
+    return CFFT_OK;
+}
+
+int cfft_serve_prepare(cfft_server server, int64_t count, const int64_t* lengths) {
+    if (!server || (count > 0 && !lengths)) return fail(CFFT_ERR_INVALID, "null server or lengths");
+    for (int64_t i = 0; i < count; i++) {
+        if (lengths[i] < 1) return fail(CFFT_ERR_INVALID, "every length must be >= 1");
+        cfft_plan_s* P = nullptr;
+        int rc = serve_plan(server, lengths[i], server->mode == CFFT_SERVE_DIRECT, &P);
+        if (rc) return rc;
+    }
+    return CFFT_OK;
+}
+
+int cfft_serve_submit(cfft_server server, int64_t n, const void* d_in, void* d_out, int direction,
+                      int64_t* ticket) {
+    if (!server || !d_in || !d_out || !ticket) return fail(CFFT_ERR_INVALID, "null server, buffer or ticket");
+    if (n < 1) return fail(CFFT_ERR_INVALID, "n must be >= 1");
+    if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    const size_t e = elem_bytes(server->dtype);
+    if (((uintptr_t)d_in % e) != 0 || ((uintptr_t)d_out % e) != 0)
+        return fail(CFFT_ERR_INVALID, "buffers must be aligned to the element size");
+    cfft_server_s* S = server;
+    cfft_plan_s* P = nullptr;
+    if (S->mode == CFFT_SERVE_DIRECT) {
+        int rc = serve_plan(S, n, true, &P);
+        if (rc) return rc;
+    }
+    const int64_t t = S->next.fetch_add(1);
+    if (t >= S->capacity) {
+        S->next.fetch_sub(1);
+        return fail(CFFT_ERR_NOMEM, "request table full (max_requests)");
+    }
+    ServeReq& r = S->req[t];
+    r.n = n;
+    r.in = d_in;
+    r.out = d_out;
+    r.dir = direction;
+    r.t_done = 0;
+    r.state.store(0);
+    r.t_sub = now_us();
+    if (S->mode == CFFT_SERVE_DIRECT) {
+        std::lock_guard<std::mutex> lk(S->qmu);
+        const size_t need = serve_scratch(P);
+        if (need > S->dscratch_cap) {
+            if (S->dscratch) {
+                cudaStreamSynchronize(S->dstream);
+                cudaFree(S->dscratch);
+            }
+            S->dscratch = nullptr;
+            S->dscratch_cap = 0;
+            CUDA_TRY(cudaMalloc(&S->dscratch, need));
+            S->dscratch_cap = need;
+        }
+        P->scratch[0] = S->dscratch;
+        P->scratch[1] = (char*)S->dscratch + need / 2;
+        int rc = plan_execute(P, d_in, d_out, direction, S->dstream, -1);
+        if (rc) {
+            r.state.store(-rc);
+            S->done++;
+            return rc;
+        }
+        cudaEvent_t ev;
+        if (!S->evpool.empty()) {
+            ev = S->evpool.back();
+            S->evpool.pop_back();
+        } else {
+            CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        }
+        CUDA_TRY(cudaEventRecord(ev, S->dstream));
+        r.state.store(1);
+        S->dpending.push_back({t, ev});
+        S->launches += (int64_t)P->stages.size();
+    } else {
+        std::lock_guard<std::mutex> lk(S->qmu);
+        S->queue.push_back(t);
+    }
+    S->qcv.notify_one();
+    *ticket = t;
+    return CFFT_OK;
+}
+
+static int serve_status(cfft_server_s* S, int64_t t, double* latency_us) {
+    const int st = S->req[t].state.load();
+    if (st < 0) {
+        std::lock_guard<std::mutex> lk(S->emu);
+        return fail(-st, S->errmsg.empty() ? "request failed" : S->errmsg);
+    }
+    if (latency_us) *latency_us = S->req[t].t_done - S->req[t].t_sub;
+    return CFFT_OK;
+}
+
+int cfft_serve_query(cfft_server server, int64_t ticket, int* done, double* latency_us) {
+    if (!server || !done) return fail(CFFT_ERR_INVALID, "null server or flag");
+    if (ticket < 0 || ticket >= server->next.load()) return fail(CFFT_ERR_INVALID, "unknown ticket");
+    const int st = server->req[ticket].state.load();
+    *done = (st == 2 || st < 0) ? 1 : 0;
+    if (!*done) return CFFT_OK;
+    return serve_status(server, ticket, latency_us);
+}
+
+int cfft_serve_wait(cfft_server server, int64_t ticket, double* latency_us) {
+    if (!server) return fail(CFFT_ERR_INVALID, "null server");
+    if (ticket < 0 || ticket >= server->next.load()) return fail(CFFT_ERR_INVALID, "unknown ticket");
+    {
+        std::unique_lock<std::mutex> lk(server->dmu);
+        server->dcv.wait(lk, [&] {
+            const int st = server->req[ticket].state.load();
+            return st == 2 || st < 0;
+        });
+    }
+    return serve_status(server, ticket, latency_us);
+}
+
+int cfft_serve_drain(cfft_server server) {
+    if (!server) return fail(CFFT_ERR_INVALID, "null server");
+    const int64_t n = server->next.load();
+    {
+        std::unique_lock<std::mutex> lk(server->dmu);
+        server->dcv.wait(lk, [&] { return server->done.load() >= n; });
+    }
+    for (int64_t t = 0; t < n; t++)
+        if (server->req[t].state.load() < 0) return serve_status(server, t, nullptr);
+    return CFFT_OK;
+}
+
+int cfft_serve_stats(cfft_server server, int64_t* requests, int64_t* batches, int64_t* launches) {
+    if (!server) return fail(CFFT_ERR_INVALID, "null server");
+    if (requests) *requests = server->next.load();
+    if (batches) *batches = server->batches.load();
+    if (launches) *launches = server->launches.load();
+    return CFFT_OK;
+}
+
+int cfft_serve_destroy(cfft_server server) {
+    if (!server) return fail(CFFT_ERR_INVALID, "null server");
+    serve_free(server);
+    delete server;
+    return CFFT_OK;
+}

@@ -118,6 +118,48 @@ int cfft_batch_destroy(cfft_batch batch);
 int64_t cfft_batch_elements(cfft_batch batch);
 int cfft_batch_launches(cfft_batch batch);
 
+/* Serving form: requests of any length arrive one at a time, from any host
+ * thread, with device buffers; the reference runs each call to completion on
+ * the calling thread (fft/ifft/bfft, src/CatabraFFT.jl:65-115).
+ *   CFFT_SERVE_BATCHED  a worker thread batches whatever is queued whenever a
+ *                       launch slot is idle (continuous batching), admitting
+ *                       requests in arrival order while the bytes in flight
+ *                       (input + output + two-pass scratch) stay under
+ *                       max_inflight_bytes (0: 64 GiB);
+ *   CFFT_SERVE_DIRECT   every request launches on arrival through its own
+ *                       cached plan (the per-request path, for comparison).
+ * A request's result is the same whichever requests share its batch.
+ * max_requests bounds the tickets of the server's lifetime (0: 2^18).
+ * Buffers must stay valid until the request completes. */
+typedef struct cfft_server_s* cfft_server;
+enum { CFFT_SERVE_BATCHED = 0, CFFT_SERVE_DIRECT = 1 };
+int cfft_serve_create(cfft_server* server, int dtype, int64_t max_inflight_bytes, int64_t max_requests,
+                      int mode);
+
+/* Builds the plans of these lengths ahead of traffic (plan_fft for each). */
+int cfft_serve_prepare(cfft_server server, int64_t count, const int64_t* lengths);
+
+/* Queues one transform of length n (direction as cfft_execute); returns its
+ * ticket.  Lengths without a plan are planned on first use. */
+int cfft_serve_submit(cfft_server server, int64_t n, const void* d_in, void* d_out, int direction,
+                      int64_t* ticket);
+
+/* *done = 1 once the request has finished (its status is then returned and
+ * latency_us, if not null, receives completion - submission in microseconds). */
+int cfft_serve_query(cfft_server server, int64_t ticket, int* done, double* latency_us);
+
+/* Blocks until the request finishes; status and latency as cfft_serve_query. */
+int cfft_serve_wait(cfft_server server, int64_t ticket, double* latency_us);
+
+/* Blocks until every submitted request has finished. */
+int cfft_serve_drain(cfft_server server);
+
+/* Requests submitted, batches formed, kernel launches issued so far. */
+int cfft_serve_stats(cfft_server server, int64_t* requests, int64_t* batches, int64_t* launches);
+
+/* Finishes queued requests, stops the worker and releases everything. */
+int cfft_serve_destroy(cfft_server server);
+
 /* No counterpart in the reference.  The two-pass FFT for callers that cannot
  * allocate device memory (an allocator-owned or capture-time context): the
  * scratch and twiddle tables live in one fixed __device__ array (32 MiB +

@@ -45,6 +45,16 @@ def test_invalid_arguments_return_status():
     assert lib.cfft_execute(None, None, None, 0, None) == m._lib.ERR_INVALID
     assert lib.cfft_plan_destroy(None) == m._lib.ERR_INVALID
     assert lib.cfft_plan_launches(None) == -1
+    srv = ctypes.c_void_p()
+    assert lib.cfft_serve_create(ctypes.byref(srv), 5, 0, 0, 0) == m._lib.ERR_INVALID
+    assert lib.cfft_serve_create(ctypes.byref(srv), 0, 0, 0, 9) == m._lib.ERR_INVALID
+    assert lib.cfft_serve_create(None, 0, 0, 0, 0) == m._lib.ERR_INVALID
+    t = ctypes.c_int64()
+    assert lib.cfft_serve_submit(None, 16, None, None, 0, ctypes.byref(t)) == m._lib.ERR_INVALID
+    assert lib.cfft_serve_wait(None, 0, None) == m._lib.ERR_INVALID
+    assert lib.cfft_serve_drain(None) == m._lib.ERR_INVALID
+    assert lib.cfft_serve_destroy(None) == m._lib.ERR_INVALID
+    assert lib.cfft_batch_create(None, 1, None, 0, 0) == m._lib.ERR_INVALID
 
 
 def test_python_api_argument_errors():

@@ -1,0 +1,114 @@
+"""GPU tests of the serving form (cfft_serve_*).
+
+* Every request's result is bit-for-bit the same whether it runs alone or in
+  a mixed micro-batch with other lengths and directions.
+* Results match the single-plan path: 1e-12 relative L2 for ComplexF64,
+  1e-5 against the FP64 oracle for ComplexF32.
+* The direct (per-request) mode matches the oracle too, and a tiny admission
+  cap still completes every request.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+import oracle
+from _pkg import load
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def cb():
+    import torch
+    assert torch.cuda.is_available()
+    return load()
+
+
+def _requests(count, seed, hi):
+    w = importlib.import_module("catabra_b200.workloads")
+    return [n for _, n in w.request_stream(count, 50000.0, seed=seed, lo=64, hi=hi)]
+
+
+def _inputs(lengths, dtype, seed):
+    import torch
+    rng = np.random.default_rng(seed)
+    xs = [(rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(dtype) for n in lengths]
+    return xs, [torch.from_numpy(x).cuda() for x in xs]
+
+
+def _run(cb, dtype, lengths, xd, dirs, together, mode=None, cap=0):
+    import torch
+    srv = cb.Server(dtype, mode=cb.SERVE_BATCHED if mode is None else mode, max_inflight_bytes=cap)
+    srv.prepare(sorted(set(lengths)))
+    ys = [torch.empty_like(x) for x in xd]
+    if together:
+        ts = [srv.submit(x, y, d) for x, y, d in zip(xd, ys, dirs)]
+        lat = [srv.wait(t) for t in ts]
+    else:
+        lat = [srv.wait(srv.submit(x, y, d)) for x, y, d in zip(xd, ys, dirs)]
+    st = srv.stats()
+    srv.close()
+    assert all(v >= 0 for v in lat)
+    return [y.cpu().numpy() for y in ys], st
+
+
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_alone_equals_in_mix(cb, dtype):
+    lengths = _requests(48, seed=3, hi=1 << 20)
+    dirs = [i % 3 for i in range(len(lengths))]
+    xs, xd = _inputs(lengths, dtype, seed=4)
+    mixed, st = _run(cb, dtype, lengths, xd, dirs, together=True)
+    alone, st1 = _run(cb, dtype, lengths, xd, dirs, together=False)
+    assert st["batches"] < len(lengths)           # requests did share batches
+    assert st1["batches"] == len(lengths)
+    for i, (a, b) in enumerate(zip(mixed, alone)):
+        assert np.array_equal(a, b), (i, lengths[i])
+
+
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_serve_matches_plans(cb, dtype):
+    lengths = _requests(24, seed=5, hi=1 << 21) + [4096, 30240, 10007, 65537, 1 << 22, 2656464]
+    dirs = [0] * len(lengths)
+    dirs[1] = 1
+    dirs[2] = 2
+    xs, xd = _inputs(lengths, dtype, seed=6)
+    ys, _ = _run(cb, dtype, lengths, xd, dirs, together=True)
+    tol = 1e-12 if dtype == np.complex128 else 1e-5
+    for x, y, d, n in zip(xs, ys, dirs, lengths):
+        xx = x.astype(np.complex128)
+        if dtype == np.complex64:
+            ref = (oracle.fft, oracle.ifft, oracle.bfft)[d](xx)
+        else:
+            ref = (cb.fft, cb.ifft, cb.bfft)[d](xx)
+        assert rel(y, ref) < tol, (n, d)
+
+
+def test_direct_mode_and_small_cap(cb):
+    lengths = _requests(32, seed=8, hi=1 << 20)
+    dirs = [0] * len(lengths)
+    xs, xd = _inputs(lengths, np.complex64, seed=9)
+    direct, st = _run(cb, np.complex64, lengths, xd, dirs, together=True, mode=cb.SERVE_DIRECT)
+    capped, stc = _run(cb, np.complex64, lengths, xd, dirs, together=True, cap=1 << 20)
+    for x, a, b, n in zip(xs, direct, capped, lengths):
+        ref = oracle.fft(x.astype(np.complex128))
+        assert rel(a, ref) < 1e-5, n
+        assert rel(b, ref) < 1e-5, n
+    assert stc["requests"] == len(lengths)
+
+
+def test_serve_rejects_bad_requests(cb):
+    import torch
+    srv = cb.Server(np.complex64)
+    x = torch.zeros(16, dtype=torch.complex64, device="cuda")
+    with pytest.raises(cb.CatabraError):
+        srv.submit_ptr(0, x.data_ptr(), x.data_ptr())
+    with pytest.raises(cb.CatabraError):
+        srv.submit_ptr(16, x.data_ptr(), x.data_ptr(), direction=5)
+    with pytest.raises(cb.CatabraError):
+        srv.wait(123)
+    srv.close()
