@@ -79,8 +79,10 @@ __device__ __forceinline__ double2 tw_two(const TwoLevel& t, unsigned e) {
 __device__ __forceinline__ double2 apply_tw(double2 v, const TwoLevel& t, unsigned e) {
     return e ? cmul(v, tw_two(t, e)) : v;
 }
+// ComplexF32: the twiddle is formed in FP64 and rounded once to FP32, then
+// applied in FP32 (the data never leaves FP32)
 __device__ __forceinline__ float2 apply_tw(float2 v, const TwoLevel& t, unsigned e) {
-    return e ? fromd<float2>(cmul(tod(v), tw_two(t, e))) : v;
+    return e ? cmul(v, fromd<float2>(tw_two(t, e))) : v;
 }
 
 // block index within this parameter block's launch (batched launches run many
@@ -711,64 +713,98 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
 
 // ------------------------------------------------------- COLPASS / ROWPASS
 // COLPASS: tile of V adjacent columns c0..c0+V of the N1 x N2 view of one
-// transform; column FFTs; store w^(i2 k1)-scaled result to scratch row-major.
-template <typename V, int EMAX>
-__device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* smem) {
+// transform; column FFTs; store the w^(i2 k1)-scaled result to scratch
+// row-major.  ROWPASS: tile of V adjacent rows r0..r0+V of the scratch; row
+// FFTs; store X[k1 + N1 k2] (natural order), optionally with the Bluestein
+// epilogue.  A tile streams into shared memory with cp.async (all of its
+// copies in flight at once); pre-multiplications (conjugation, chirp,
+// spectrum) are applied in shared memory once it has arrived.  The
+// sub-transform twiddle table is staged in shared memory when small.
+template <typename V>
+__device__ __forceinline__ void colpass_issue(const KParams& p, int tile, V* dst) {
     const int T = blockDim.x, tid = opaque_tid();
-    const int tiles = p.N2 / p.V;
-    const int b = block_id(p);
-    const int t = b / tiles, c0 = (b - t * tiles) * p.V;
-    if (t >= p.batch) return;
-    V* buf = (V*)smem;
+    const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
     const V* in = (const V*)p.in + (long long)t * p.in_dist;
-    V* out = (V*)p.out + (long long)t * p.out_dist;
-    const int N1 = p.N1, N2 = p.N2, Vw = p.V;
-    for (int idx = tid; idx < N1 * Vw; idx += T) {
+    const int N2 = p.N2, Vw = p.V, PA = p.PA, total = p.N1 * Vw;
+    const long long lim = (p.pre == PRE_CHIRP) ? (long long)p.nx : (1LL << 62);
+    for (int idx = tid; idx < total; idx += T) {
         const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
         const long long jj = (long long)i1 * N2 + c0 + j;
-        V v;
-        if (p.pre == PRE_CHIRP) {
-            v = zero<V>();
-            if (jj < p.nx) v = fromd<V>(cmul(tod(load_in(p, ldg_stream(in + jj))), __ldg(p.chirp + jj)));
-        } else if (p.pre == PRE_SPEC) {
-            v = conjv(fromd<V>(cmul(tod(ldg_stream(in + jj)), __ldg(p.spec + jj))));
-        } else {
-            v = load_in(p, ldg_stream(in + jj));
-        }
-        buf[i1 * p.PA + j] = v;
+        if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
     }
-    __syncthreads();
-    run_subffts<V, EMAX>(buf, p.pa, Vw, p.PA, 1);
-    for (int idx = tid; idx < N1 * Vw; idx += T) {
-        const int k1 = fdiv(idx, p.mV), j = idx - k1 * Vw;
-        const unsigned e = (unsigned)((unsigned long long)(c0 + j) * k1 % (unsigned long long)p.M);
-        out[(long long)k1 * N2 + c0 + j] = apply_tw(buf[k1 * p.PA + j], p.t4, e);
+}
+// prologue on the arrived tile; returns whether it wrote (caller syncs)
+template <typename V>
+__device__ __forceinline__ bool colpass_fix(const KParams& p, int tile, V* buf) {
+    if (p.pre == PRE_NONE && !p.dir) return false;
+    const int T = blockDim.x, tid = opaque_tid();
+    const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
+    const int N2 = p.N2, Vw = p.V, PA = p.PA, total = p.N1 * Vw;
+#pragma unroll 4
+    for (int idx = tid; idx < total; idx += T) {
+        const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
+        const long long jj = (long long)i1 * N2 + c0 + j;
+        V* e = buf + i1 * PA + j;
+        if (p.pre == PRE_NONE) {
+            *e = conjv(*e);
+        } else if (p.pre == PRE_CHIRP) {
+            *e = (jj < p.nx) ? fromd<V>(cmul(tod(load_in(p, *e)), __ldg(p.chirp + jj))) : zero<V>();
+        } else {
+            *e = conjv(fromd<V>(cmul(tod(*e), __ldg(p.spec + jj))));
+        }
+    }
+    return true;
+}
+// column FFTs and the twiddled store; (c0 + j) * k1 < N2 * N1 = M, so the
+// exponent needs no reduction
+template <typename V, int EMAX>
+__device__ __forceinline__ void colpass_finish(const KParams& p, int tile, V* buf, const V* tw) {
+    const int T = blockDim.x, tid = opaque_tid();
+    const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
+    V* out = (V*)p.out + (long long)t * p.out_dist;
+    const int N1 = p.N1, N2 = p.N2, Vw = p.V, PA = p.PA, total = N1 * Vw;
+    run_subffts<V, EMAX, 2>(buf, p.pa, tw, Vw, PA, 1);
+    if (T % Vw == 0) {
+        // each thread keeps one column: no per-element division
+        const int j = tid % Vw, ks = T / Vw;
+        const unsigned c = (unsigned)(c0 + j);
+        V* o = out + c0 + j;
+#pragma unroll 4
+        for (int k1 = tid / Vw; k1 < N1; k1 += ks)
+            o[(long long)k1 * N2] = apply_tw(buf[k1 * PA + j], p.t4, c * (unsigned)k1);
+    } else {
+#pragma unroll 4
+        for (int idx = tid; idx < total; idx += T) {
+            const int k1 = fdiv(idx, p.mV), j = idx - k1 * Vw;
+            const unsigned e = (unsigned)(c0 + j) * (unsigned)k1;
+            out[(long long)k1 * N2 + c0 + j] = apply_tw(buf[k1 * PA + j], p.t4, e);
+        }
     }
 }
 
-// ROWPASS: tile of V adjacent rows r0..r0+V of the scratch; row FFTs; store
-// X[k1 + N1 k2] (natural order), optionally with the Bluestein epilogue.
-template <typename V, int EMAX>
-__device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* smem) {
+template <typename V>
+__device__ __forceinline__ void rowpass_issue(const KParams& p, int tile, V* dst) {
     const int T = blockDim.x, tid = opaque_tid();
-    const int tiles = p.N1 / p.V;
-    const int b = block_id(p);
-    const int t = b / tiles, r0 = (b - t * tiles) * p.V;
-    if (t >= p.batch) return;
-    V* buf = (V*)smem;
-    const V* in = (const V*)p.in + (long long)t * p.in_dist;
-    V* out = (V*)p.out + (long long)t * p.out_dist;
-    const int N1 = p.N1, N2 = p.N2, Vw = p.V;
-    for (int idx = tid; idx < Vw * N2; idx += T) {
+    const int tiles = p.N1 / p.V, t = tile / tiles, r0 = (tile - t * tiles) * p.V;
+    const int N2 = p.N2, PC = p.PC;
+    const V* src = (const V*)p.in + (long long)t * p.in_dist + (long long)r0 * N2;
+    for (int idx = tid; idx < p.V * N2; idx += T) {
         const int r = fdiv(idx, p.mN2), i2 = idx - r * N2;
-        buf[r * p.PC + i2] = in[(long long)(r0 + r) * N2 + i2];
+        cp_async_elem(dst + r * PC + i2, src + idx);
     }
-    __syncthreads();
-    run_subffts<V, EMAX>(buf, p.pc, Vw, 1, p.PC);
+}
+template <typename V, int EMAX>
+__device__ __forceinline__ void rowpass_finish(const KParams& p, int tile, V* buf, const V* tw) {
+    const int T = blockDim.x, tid = opaque_tid();
+    const int tiles = p.N1 / p.V, t = tile / tiles, r0 = (tile - t * tiles) * p.V;
+    V* out = (V*)p.out + (long long)t * p.out_dist;
+    const int N1 = p.N1, N2 = p.N2, Vw = p.V, PC = p.PC;
+    run_subffts<V, EMAX, 2>(buf, p.pc, tw, Vw, 1, PC);
+#pragma unroll 4
     for (int idx = tid; idx < Vw * N2; idx += T) {
         const int k2 = fdiv(idx, p.mV), r = idx - k2 * Vw;
         const long long k = (long long)(r0 + r) + (long long)N1 * k2;
-        V v = buf[r * p.PC + k2];
+        V v = buf[r * PC + k2];
         if (p.post == POST_CHIRP) {
             if (k < p.nx)
                 stg_stream(out + k, store_out(p, fromd<V>(cmul(tod(conjv(v)), __ldg(p.chirp + k)))));
@@ -778,4 +814,37 @@ __device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* sm
             stg_stream(out + k, store_out(p, v));
         }
     }
+}
+
+// one tile per CTA
+template <typename V, int EMAX>
+__device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* smem) {
+    const int T = blockDim.x, tid = opaque_tid();
+    const int tile = block_id(p);
+    if (tile >= p.batch * (p.N2 / p.V)) return;
+    const int lt = cfft_pass_tw_elems(p.pa.twlen, (int)sizeof(V));
+    V* tws = (V*)smem;
+    V* buf = tws + lt;
+    colpass_issue<V>(p, tile, buf);
+    cp_async_commit();
+    for (int i = tid; i < lt; i += T) tws[i] = ((const V*)p.pa.tw)[i];
+    cp_async_wait_all();
+    __syncthreads();
+    if (colpass_fix<V>(p, tile, buf)) __syncthreads();
+    colpass_finish<V, EMAX>(p, tile, buf, lt ? (const V*)tws : (const V*)p.pa.tw);
+}
+template <typename V, int EMAX>
+__device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* smem) {
+    const int T = blockDim.x, tid = opaque_tid();
+    const int tile = block_id(p);
+    if (tile >= p.batch * (p.N1 / p.V)) return;
+    const int lt = cfft_pass_tw_elems(p.pc.twlen, (int)sizeof(V));
+    V* tws = (V*)smem;
+    V* buf = tws + lt;
+    rowpass_issue<V>(p, tile, buf);
+    cp_async_commit();
+    for (int i = tid; i < lt; i += T) tws[i] = ((const V*)p.pc.tw)[i];
+    cp_async_wait_all();
+    __syncthreads();
+    rowpass_finish<V, EMAX>(p, tile, buf, lt ? (const V*)tws : (const V*)p.pc.tw);
 }

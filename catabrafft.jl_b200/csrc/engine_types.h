@@ -68,6 +68,16 @@ struct KParams {
     long long in_off, out_off;    // batched launches: element offsets added to the bases
 };
 
+// COLPASS / ROWPASS stage their sub-transform twiddle table in shared memory
+// (ahead of the tile) when it is small; larger tables are read from L2.
+// Host and device use this one rule to agree on the shared-memory size.
+inline __host__ __device__ bool cfft_pass_tw_staged(int twlen, int elem_bytes) {
+    return twlen > 0 && twlen * elem_bytes <= 16384;
+}
+inline __host__ __device__ int cfft_pass_tw_elems(int twlen, int elem_bytes) {
+    return cfft_pass_tw_staged(twlen, elem_bytes) ? twlen : 0;
+}
+
 // One launch of the batched executor: parameter blocks in device memory and,
 // per block of the grid, the index of its parameter block.
 struct BatchLaunch {

@@ -18,13 +18,18 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_four(KPar
     extern __shared__ __align__(16) unsigned char smem[];
     four_body<V, EMAX, K>(p, smem);
 }
+// the pass kernels keep three ComplexF32 CTAs resident per SM (80 registers
+// suffice for their radix-16 codelets)
+template <typename V> struct PassBlocks { static constexpr int value = 3; };
+template <> struct PassBlocks<double2> { static constexpr int value = 2; };
+
 template <typename V, int EMAX>
-__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_colpass(KParams p) {
+__global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) k_colpass(KParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     colpass_body<V, EMAX>(p, smem);
 }
 template <typename V, int EMAX>
-__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_rowpass(KParams p) {
+__global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) k_rowpass(KParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     rowpass_body<V, EMAX>(p, smem);
 }
@@ -61,13 +66,13 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_four(Bat
 }
 
 template <typename V, int EMAX>
-__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_colpass(BatchLaunch L) {
+__global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) kb_colpass(BatchLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ KParams sp;
     colpass_body<V, EMAX>(stage_params<V>(L, &sp), smem);
 }
 template <typename V, int EMAX>
-__global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_rowpass(BatchLaunch L) {
+__global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) kb_rowpass(BatchLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ KParams sp;
     rowpass_body<V, EMAX>(stage_params<V>(L, &sp), smem);

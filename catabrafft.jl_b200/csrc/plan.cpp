@@ -21,6 +21,7 @@
 #include <deque>
 #include <thread>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -421,8 +422,9 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
         v.push_back(sh);
     }
     if (M > 64) four_candidates(M, n, conv, dtype, v);
-    if (v.empty()) {
-        // beyond a cluster: two HBM passes; Rader here becomes Bluestein
+    if (v.empty() || M >= 16384) {
+        // beyond a cluster (or as the timed planners' alternative to one):
+        // two HBM passes; Rader here becomes Bluestein
         int c2 = conv;
         int64_t M2 = M;
         if (conv == CONV_RADER) { c2 = CONV_BLUE; M2 = smooth_ceil(2 * n - 1); }
@@ -432,7 +434,9 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
         for (int tries = 0; tries < 256; tries++) {
             if (global_shape(M2, dtype, g)) {
                 g.conv = c2;
-                v.push_back(g);
+                // second in line: the heuristic keeps a single-kernel shape
+                // first, MEASURE and ENCHANT always time this one
+                v.insert(v.begin() + std::min<size_t>(v.size(), 1), g);
                 break;
             }
             if (c2 == CONV_NONE) break;
@@ -512,8 +516,13 @@ template <class T> static void put(std::vector<unsigned char>& img, const std::v
     memcpy(img.data(), v.data(), img.size());
 }
 
+// prefer_block: keep the block-wide team whenever its lanes span at least
+// 128 bytes of adjacent sub-transforms (conflict-free shared-memory access in
+// both the column layout, sub-transforms adjacent, and the row layout, odd
+// pitch); warp-owned sub-transforms walk one sub-transform with a stride and
+// collide on the banks when that stride is an even multiple of 128 bytes
 static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, int64_t count,
-                        SubPlan& sp) {
+                        SubPlan& sp, bool prefer_block = false) {
     memset(&sp, 0, sizeof sp);
     sp.L = (int)L;
     sp.np = (int)rad.size();
@@ -532,6 +541,7 @@ static int make_subplan(cfft_plan_s* P, int64_t L, const std::vector<int>& rad, 
     if (gw > 1 << 16) gw = 1 << 16;
     sp.Gwarp = 0;
     if (gw >= 1 && count >= (int64_t)(CFFT_THREADS / 32) * gw / 2) sp.Gwarp = gw;
+    if (prefer_block && std::min<int64_t>(sp.G, count) * (int64_t)elem_bytes(P->dtype) >= 128) sp.Gwarp = 0;
     if (L <= 1) { sp.tw = nullptr; sp.twlen = 0; return CFFT_OK; }
     // per-pass blocks: pass (r, s), n1 = L/(s r): tw[off + (j-1) n1 + q] = w_L^(j q s)
     sp.twlen = (int)twiddle_len(L, rad);
@@ -755,9 +765,9 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         kp.mN2 = magic(sh.N2);
         kp.mR1 = magic(sh.N1 / sh.C);
         kp.mX = magic(std::max(kp.XP, 1));
-        rc = make_subplan(P, sh.N1, sh.ra, sh.N2 / sh.C, kp.pa);
+        rc = make_subplan(P, sh.N1, sh.ra, sh.N2 / sh.C, kp.pa, P->dtype == CFFT_C64);
         if (rc) return rc;
-        rc = make_subplan(P, sh.N2, sh.rc, sh.N1 / sh.C, kp.pc);
+        rc = make_subplan(P, sh.N2, sh.rc, sh.N1 / sh.C, kp.pc, P->dtype == CFFT_C64);
         if (rc) return rc;
         rc = make_twolevel(P, sh.M, kp.t4);
         if (rc) return rc;
@@ -799,17 +809,25 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     // two HBM passes per FFT_M (and two FFT_M for a convolution)
     const int64_t N1 = sh.N1, N2 = sh.N2, M = sh.M;
     const int64_t PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
-    auto pick_tile = [&](int64_t count, int64_t per) {
-        int64_t best = 1;
-        for (int64_t v = 1; v <= count; v++)
-            if (count % v == 0 && (size_t)(v * per) * e <= 96 * 1024 && v <= 64) best = v;
-        return best;
+    // tile width V: a divisor of the tile count; prefer a power of two (it
+    // divides the block, so each thread keeps one column in the epilogue)
+    // whose V-element global segments span at least 128 bytes, else the
+    // widest that fits.  ComplexF32 pass kernels run three CTAs per SM.
+    auto pick_tile = [&](int64_t count, int64_t per, size_t limit) {
+        int64_t best = 1, best2 = 0;
+        for (int64_t v = 1; v <= count; v++) {
+            if (count % v || (size_t)(v * per) * e > limit || v > 64) continue;
+            best = v;
+            if ((v & (v - 1)) == 0 && (size_t)v * e >= 128) best2 = v;
+        }
+        return best2 ? best2 : best;
     };
-    const int64_t Vc = pick_tile(N2, N1), Vr = pick_tile(N1, PC);
+    const size_t tile_lim = (e == 8) ? 72 * 1024 : 96 * 1024;
+    const int64_t Vc = pick_tile(N2, N1, tile_lim), Vr = pick_tile(N1, PC, tile_lim);
     SubPlan pa, pc;
-    rc = make_subplan(P, N1, sh.ra, Vc, pa);
+    rc = make_subplan(P, N1, sh.ra, Vc, pa, true);
     if (rc) return rc;
-    rc = make_subplan(P, N2, sh.rc, Vr, pc);
+    rc = make_subplan(P, N2, sh.rc, Vr, pc, true);
     if (rc) return rc;
     TwoLevel t4;
     rc = make_twolevel(P, M, t4);
@@ -839,7 +857,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp.t4 = t4;
         s.kp.pre = pre;
         s.threads = CFFT_THREADS;
-        s.smem = (size_t)(N1 * Vc) * e + 16;
+        s.smem = (size_t)(cfft_pass_tw_elems(pa.twlen, (int)e) + N1 * Vc) * e + 16;
         s.cluster = 1;
         s.in_sel = in_sel;
         s.out_sel = out_sel;
@@ -858,7 +876,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp.pc = pc;
         s.kp.post = post;
         s.threads = CFFT_THREADS;
-        s.smem = (size_t)(Vr * PC) * e + 16;
+        s.smem = (size_t)(cfft_pass_tw_elems(pc.twlen, (int)e) + Vr * PC) * e + 16;
         s.cluster = 1;
         s.in_sel = in_sel;
         s.out_sel = out_sel;
@@ -990,10 +1008,18 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
         cudaMemset(buf, 0, (size_t)n * batch * e);
         float best = 1e30f;
         int best_i = -1;
+        const char* logenv = getenv("CFFT_TUNE_LOG");      // diagnostics: one line per candidate
+        const bool log = logenv && logenv[0] == '1';
         for (size_t i = 0; i < limit; i++) {
             if (plan_build(P, cands[i]) == CFFT_OK) {
                 float t = time_plan(P, buf);
+                if (log)
+                    fprintf(stderr, "cfft-tune n=%lld batch=%lld %s smem=%zu co-resident=%d %.4f ms\n",
+                            (long long)n, (long long)batch, P->desc.c_str(), P->stages[0].smem,
+                            P->stages[0].max_units, t);
                 if (t < best) { best = t; best_i = (int)i; }
+            } else if (log) {
+                fprintf(stderr, "cfft-tune n=%lld candidate %zu failed: %s\n", (long long)n, i, g_err);
             }
             plan_free(P);
         }
