@@ -434,9 +434,12 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
         for (int tries = 0; tries < 256; tries++) {
             if (global_shape(M2, dtype, g)) {
                 g.conv = c2;
-                // second in line: the heuristic keeps a single-kernel shape
-                // first, MEASURE and ENCHANT always time this one
-                v.insert(v.begin() + std::min<size_t>(v.size(), 1), g);
+                // measured on B200: for ComplexF32 transforms of 2^15 points
+                // and more the two passes beat a cluster (1.3-1.5x at
+                // 2^16-2^17); otherwise second in line, so the heuristic
+                // keeps a single-kernel shape and MEASURE/ENCHANT time both
+                const bool first = dtype == CFFT_C64 && conv == CONV_NONE && M >= 32768;
+                v.insert(v.begin() + (first ? 0 : std::min<size_t>(v.size(), 1)), g);
                 break;
             }
             if (c2 == CONV_NONE) break;

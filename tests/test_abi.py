@@ -77,6 +77,14 @@ def test_strategy_choice(n, expect):
     assert expect in m.describe_strategy(n), m.describe_strategy(n)
 
 
+@pytest.mark.parametrize("n,expect", [
+    (65536, "twopass(N1=256,N2=256)"), (19683, "four(C="), (4096, "rows"),
+])
+def test_strategy_choice_complex64(n, expect):
+    m = load()
+    assert expect in m.describe_strategy(n, np.complex64), m.describe_strategy(n, np.complex64)
+
+
 def test_strategy_covers_every_length_class():
     # every n in the batching/serving range maps to some strategy
     m = load()
