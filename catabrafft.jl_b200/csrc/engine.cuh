@@ -376,6 +376,8 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
 // compile time for the hot sizes so strides, counts and divisions fold to
 // constants.
 template <int WM> struct DynK {
+    static constexpr bool kSingle = false;     // separate column and row buffers
+    static constexpr int kNEf = 1, kNEi = 1;
     __device__ static int N1(const KParams& p) { return p.N1; }
     __device__ static int N2(const KParams& p) { return p.N2; }
     __device__ static int C(const KParams& p) { return p.C; }
@@ -423,8 +425,14 @@ __device__ __forceinline__ void st_subffts(V* buf, const V* tw, Seq<R...>) {
     if constexpr (WARP) __syncthreads();
 }
 
-template <int N1_, int N2_, int C_, class SA, bool WA, int GA, class SC, bool WC, int GC>
+// SB: one shared buffer for both layouts; the exchange stages each thread's
+// share in registers between two cluster barriers (FOUR kernels run 256
+// threads, so a thread holds ceil(elements / 256) of them)
+template <int N1_, int N2_, int C_, class SA, bool WA, int GA, class SC, bool WC, int GC, bool SB = false>
 struct StatK {
+    static constexpr bool kSingle = SB;
+    static constexpr int kNEf = (N1_ * (N2_ / C_) + 255) / 256;
+    static constexpr int kNEi = ((N1_ / C_) * N2_ + 255) / 256;
     static constexpr int kW = N2_ / C_, kR1 = N1_ / C_;
     static constexpr int kPC = N2_ + ((N2_ % 2 == 0) ? 1 : 0);
     static constexpr int kPA = (C_ == 1) ? kPC : kW;
@@ -480,6 +488,70 @@ __device__ __forceinline__ void four_push_inv(const KParams& p, V* bufA, const V
         const int k1 = c * R1 + r, d = K::dW(p, i2);
         V* dst = cl.map_shared_rank(bufA, d);
         dst[k1 * PA + (i2 - d * W)] = apply_tw(bufC[r * PC + i2], t4, (unsigned)(i2 * k1));
+    }
+    cl.sync();
+}
+
+// Single-buffer exchanges (K::kSingle): each thread reads its elements of the
+// source layout, twiddled, into registers; a cluster barrier (every CTA has
+// read its own buffer); remote stores into the owners' buffers in the target
+// layout; a cluster barrier publishes them.  Halving the shared memory lets
+// the hot shapes run on half as many, twice as large CTAs at two CTAs/SM.
+template <typename V, class K>
+__device__ __forceinline__ void four_push_fwd_sb(const KParams& p, V* buf, cg::cluster_group& cl,
+                                                 unsigned c, const TwoLevel& t4) {
+    constexpr int NE = K::kNEf;
+    const int W = K::W(p), R1 = K::R1(p), PA = K::PA(p), PC = K::PC(p);
+    const int tid = opaque_tid();
+    const int total = K::N1(p) * W;
+    V v[NE];
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        const int idx = tid + m * 256;
+        if (idx < total) {
+            const int k1 = K::dW(p, idx), j = idx - k1 * W;
+            v[m] = apply_tw(buf[k1 * PA + j], t4, (unsigned)((c * W + j) * k1));
+        }
+    }
+    cl.sync();
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        const int idx = tid + m * 256;
+        if (idx < total) {
+            const int k1 = K::dW(p, idx), j = idx - k1 * W;
+            const int i2 = c * W + j, d = K::dR1(p, k1);
+            V* dst = cl.map_shared_rank(buf, d);
+            dst[(k1 - d * R1) * PC + i2] = v[m];
+        }
+    }
+    cl.sync();
+}
+template <typename V, class K>
+__device__ __forceinline__ void four_push_inv_sb(const KParams& p, V* buf, cg::cluster_group& cl,
+                                                 unsigned c, const TwoLevel& t4) {
+    constexpr int NE = K::kNEi;
+    const int W = K::W(p), R1 = K::R1(p), N2 = K::N2(p), PA = K::PA(p), PC = K::PC(p);
+    const int tid = opaque_tid();
+    const int total = R1 * N2;
+    V v[NE];
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        const int idx = tid + m * 256;
+        if (idx < total) {
+            const int r = K::dN2(p, idx), i2 = idx - r * N2;
+            v[m] = apply_tw(buf[r * PC + i2], t4, (unsigned)(i2 * (c * R1 + r)));
+        }
+    }
+    cl.sync();
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        const int idx = tid + m * 256;
+        if (idx < total) {
+            const int r = K::dN2(p, idx), i2 = idx - r * N2;
+            const int k1 = c * R1 + r, d = K::dW(p, i2);
+            V* dst = cl.map_shared_rank(buf, d);
+            dst[k1 * PA + (i2 - d * W)] = v[m];
+        }
     }
     cl.sync();
 }
@@ -608,7 +680,8 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
 
     // ---- forward FFT_M: columns, twiddle + exchange, rows (buf = column layout)
     K::template colA<V, EMAX>(buf, p, twA);
-    if (C > 1) four_push_fwd<V, K>(p, buf, bufC, cl, c, t4);
+    if constexpr (K::kSingle) four_push_fwd_sb<V, K>(p, buf, cl, c, t4);
+    else if (C > 1) four_push_fwd<V, K>(p, buf, bufC, cl, c, t4);
     else four_twiddle_local<V, K>(p, buf, t4);
     K::template rowC<V, EMAX>(bufC, p, twC);
 
@@ -632,7 +705,8 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     __syncthreads();
     // ---- second FFT_M in transposed order: rows, twiddle + exchange, columns
     K::template rowC<V, EMAX>(bufC, p, twC);
-    if (C > 1) four_push_inv<V, K>(p, buf, bufC, cl, c, t4);
+    if constexpr (K::kSingle) four_push_inv_sb<V, K>(p, buf, cl, c, t4);
+    else if (C > 1) four_push_inv<V, K>(p, buf, bufC, cl, c, t4);
     else four_twiddle_local<V, K>(p, buf, t4);
     K::template colA<V, EMAX>(buf, p, twA);
     // column layout now holds conj(c[j1*N2 + c*W + j])
@@ -694,8 +768,12 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
     double2* t4lo = after16(twC + lC);
     double2* t4hi = t4lo + nlo;
     V* buf = (V*)(t4hi + nhi);            // column layout (N1 x PA)
-    V* bufC = (C > 1) ? buf + N1 * K::PA(p) : buf;   // row layout (R1 x PC)
-    V* xs = (C > 1) ? bufC + K::R1(p) * K::PC(p) : buf + N1 * K::PA(p);  // Rader x chunk
+    // row layout (R1 x PC): its own buffer, or (single buffer) the same one
+    V* bufC = (C > 1 && !K::kSingle) ? buf + N1 * K::PA(p) : buf;
+    const int lay = (C > 1) ? (K::kSingle ? max(N1 * K::PA(p), K::R1(p) * K::PC(p))
+                                          : N1 * K::PA(p) + K::R1(p) * K::PC(p))
+                            : N1 * K::PA(p);
+    V* xs = buf + lay;                    // Rader x chunk
     double2* red = after16(xs + p.XP);    // reduction scratch (32 + C entries)
 
     four_prefetch<V, K>(p, buf, t, c);

@@ -13,9 +13,10 @@
 
 // generic kernel for a mode, or nullptr
 const void* cfft_kernel_for(int mode, int dtype);
-// statically shaped FOUR kernel matching (N1, N2, C, radix multiplicities), or nullptr
+// statically shaped FOUR kernel matching (N1, N2, C, radix multiplicities), or
+// nullptr; *single (if given) = 1 when it keeps one buffer for both layouts
 const void* cfft_static_four(int dtype, int N1, int N2, int C, const unsigned char* ca,
-                             const unsigned char* cc);
+                             const unsigned char* cc, int* single = nullptr);
 cudaError_t cfft_prepare_fn(const void* fn, size_t smem, int cluster);
 cudaError_t cfft_launch_fn(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
                            int cluster, cudaStream_t stream);

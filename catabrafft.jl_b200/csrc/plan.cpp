@@ -228,6 +228,7 @@ struct Stage {
     int cluster;
     int in_sel, out_sel;     // 0 user in, 1 user out, 2 scratch0, 3 scratch1
     int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
+    size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
 };
 
 struct Shape {
@@ -237,6 +238,7 @@ struct Shape {
     int N1 = 1, N2 = 1, C = 1, V = 1;
     std::vector<int> ra, rc; // radix passes for N1 / N2 (ROWS: rc for M)
     size_t smem = 0;
+    size_t smem_dyn = 0;     // FOUR: the generic (two-buffer) kernels' shared memory
     double score = 0;
 };
 
@@ -351,8 +353,20 @@ static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vec
             }
             int64_t XP = (conv == CONV_RADER) ? (nx + C - 1) / C : 0;
             int64_t bufsz = (C == 1) ? N1 * PA : N1 * PA + R1 * PC;
-            size_t smem = four_smem_bytes(M, twiddle_len(N1, ra), twiddle_len(N2, rc), bufsz, XP, e);
-            if (smem > kSmemMax) continue;
+            const int64_t tA = twiddle_len(N1, ra), tC = twiddle_len(N2, rc);
+            // the generic kernels (and the batched forms) need this much
+            const size_t smem_dyn = four_smem_bytes(M, tA, tC, bufsz, XP, e);
+            if (smem_dyn > kSmemMax) continue;
+            // a statically shaped kernel for exactly this shape folds strides
+            // and counts to constants (preferred); a single-buffer one keeps
+            // one buffer for both layouts
+            unsigned char ca[8], cc[8];
+            radix_counts(ra, ca);
+            radix_counts(rc, cc);
+            int single = 0;
+            const bool stat = cfft_static_four(dtype, (int)N1, (int)N2, C, ca, cc, &single) != nullptr;
+            const size_t smem = (stat && single) ? four_smem_bytes(M, tA, tC, std::max(N1 * PA, R1 * PC), XP, e)
+                                                 : smem_dyn;
             Shape sh;
             sh.mode = MODE_FOUR;
             sh.conv = conv;
@@ -363,15 +377,11 @@ static void four_candidates(int64_t M, int64_t nx, int conv, int dtype, std::vec
             sh.ra = ra;
             sh.rc = rc;
             sh.smem = smem;
+            sh.smem_dyn = smem_dyn;
             double bal = std::fabs(std::log2((double)N1 / (double)N2));
             sh.score = (smem > kSmemTwoPerSM ? 8.0 : 0.0) + (C > 8 ? 3.0 : 0.0) + 0.6 * C +
                        0.5 * bal + 0.1 * (ra.size() + rc.size());
-            // a statically shaped kernel for exactly this shape folds strides
-            // and counts to constants: prefer it
-            unsigned char ca[8], cc[8];
-            radix_counts(ra, ca);
-            radix_counts(rc, cc);
-            if (cfft_static_four(dtype, (int)N1, (int)N2, C, ca, cc)) sh.score -= 6.0;
+            if (stat) sh.score -= 6.0;
             out.push_back(sh);
         }
     }
@@ -778,6 +788,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp = kp;
         s.threads = CFFT_THREADS;
         s.smem = sh.smem;
+        s.smem_batched = sh.smem_dyn;
         s.cluster = sh.C;
         s.grid = 0;
         s.in_sel = 0;
@@ -1119,6 +1130,8 @@ static int build_shared_plan(int64_t n, int dtype, int flags, int device, cfft_p
     *out = P;
     return CFFT_OK;
 }
+// shared memory of a stage's descriptor-driven (generic) kernel
+static size_t batched_smem(const Stage& st) { return st.smem_batched ? st.smem_batched : st.smem; }
 static bool single_kernel(const cfft_plan_s* P) {
     return P->stages.size() == 1 &&
            (P->stages[0].kp.mode == MODE_ROWS || P->stages[0].kp.mode == MODE_FOUR);
@@ -1216,8 +1229,8 @@ static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* leng
             kp.in_user = kp.out_user = 1;
             kp.in_dist = kp.out_dist = B->len[i];
             kp.scale = 1.0 / (double)B->len[i];
-            bins[std::make_tuple(fn, P->stages[0].cluster, smem_class(P->stages[0].smem))]
-                .push_back({i, kp, cost, P->stages[0].smem});
+            const size_t sm = batched_smem(P->stages[0]);
+            bins[std::make_tuple(fn, P->stages[0].cluster, smem_class(sm))].push_back({i, kp, cost, sm});
         } else {
             twopass.push_back(i);
         }
@@ -1468,8 +1481,8 @@ static int serve_launch(cfft_server_s* S, ServeSlot& sl) {
             kp.in_dist = kp.out_dist = r.n;
             kp.dir = r.dir;
             kp.scale = scale;
-            singles[std::make_tuple(fn, P->stages[0].cluster, smem_class(P->stages[0].smem))]
-                .push_back({kp, cost, P->stages[0].smem});
+            const size_t sm = batched_smem(P->stages[0]);
+            singles[std::make_tuple(fn, P->stages[0].cluster, smem_class(sm))].push_back({kp, cost, sm});
             continue;
         }
         const size_t one = align_up((size_t)P->shape.M * elem_bytes(S->dtype), kServeAlign);
