@@ -625,6 +625,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     V x0 = zero<V>();
     if (p.conv == CONV_NONE) {
         if (p.dir) {
+#pragma unroll 4
             for (int idx = tid; idx < N1 * W; idx += T) {
                 const int i1 = K::dW(p, idx), j = idx - i1 * W;
                 V* e = buf + i1 * PA + j;
@@ -632,6 +633,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             }
         }
     } else if (p.conv == CONV_BLUE) {
+#pragma unroll 4
         for (int idx = tid; idx < N1 * W; idx += T) {
             const int i1 = K::dW(p, idx), j = idx - i1 * W;
             const int jj = i1 * N2 + c * W + j;
@@ -661,6 +663,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             x0 = r0[0];
         }
         const int L = nx - 1;
+#pragma unroll 4
         for (int idx = tid; idx < N1 * W; idx += T) {
             const int i1 = K::dW(p, idx), j = idx - i1 * W;
             const int jj = i1 * N2 + c * W + j;
@@ -687,6 +690,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
 
     if (p.conv == CONV_NONE) {
         // X[k1 + N1 k2] from row layout (r, k2), k1 = c*R1 + r
+#pragma unroll 4
         for (int idx = tid; idx < R1 * N2; idx += T) {
             const int k2 = K::dR1(p, idx), r = idx - k2 * R1;
             stg_stream(out + (long long)(c * R1 + r) + (long long)N1 * k2,
@@ -696,6 +700,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     }
 
     // ---- pointwise multiply by spectrum/M and conjugate (inverse via conj)
+#pragma unroll 4
     for (int idx = tid; idx < R1 * N2; idx += T) {
         const int r = K::dN2(p, idx), k2 = idx - r * N2;
         const int kk = (c * R1 + r) + N1 * k2;
@@ -712,6 +717,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     // column layout now holds conj(c[j1*N2 + c*W + j])
 
     if (p.conv == CONV_BLUE) {
+#pragma unroll 4
         for (int idx = tid; idx < N1 * W; idx += T) {
             const int j1 = K::dW(p, idx), j = idx - j1 * W;
             const int jj = j1 * N2 + c * W + j;
@@ -726,6 +732,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     // Rader epilogue: y[g^-j] = x0 + c[j]; y[0] = x0 + sum(x[1:])
     const int XC = p.XP, L = nx - 1;
     if (C > 1) cl.sync(); else __syncthreads();   // everyone done reading xs
+#pragma unroll 4
     for (int idx = tid; idx < N1 * W; idx += T) {
         const int j1 = K::dW(p, idx), j = idx - j1 * W;
         const int jj = j1 * N2 + c * W + j;
