@@ -401,6 +401,9 @@ template <int... R> struct Seq {};
 template <typename V, int EMAX, bool WARP, int L, int IS, int GS, int COUNT, int GW, int S, int OFF,
           int R, int... Rest>
 __device__ __forceinline__ void st_passes(V* buf, const V* tw0) {
+    // every butterfly of a wave must have a thread slot: EMAX / R per thread
+    static_assert(GW * (L / R) <= (WARP ? 32 : 256) * (EMAX / R),
+                  "a static pass has more butterflies than its team has slots");
     const V* tw = tw0 + OFF;
     if constexpr (WARP) {
         const int nw = blockDim.x >> 5, wid = opaque_tid() >> 5;

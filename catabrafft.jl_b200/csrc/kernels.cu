@@ -18,6 +18,14 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_four(KPar
     extern __shared__ __align__(16) unsigned char smem[];
     four_body<V, EMAX, K>(p, smem);
 }
+// statically shaped variant with its own residency target: a smaller
+// per-thread element budget (EMAX) and a single shared buffer let three
+// ComplexF64 CTAs share an SM
+template <typename V, int EMAX, class K, int MB>
+__global__ void __launch_bounds__(CFFT_THREADS, MB) k_four_mb(KParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    four_body<V, EMAX, K>(p, smem);
+}
 // the pass kernels keep three ComplexF32 CTAs resident per SM (80 registers
 // suffice for their radix-16 codelets)
 template <typename V> struct PassBlocks { static constexpr int value = 3; };
@@ -159,17 +167,20 @@ using K_168x120_c8 = StatK<168, 120, 8, Seq<7, 3, 8>, true, 1, Seq<5, 3, 8>, tru
 // 30240 on a 6-CTA cluster with one shared buffer per CTA (two CTAs/SM at
 // twice the elements per CTA; 8 % faster than the 12-CTA kernel on B200)
 using K_168x180_c6s = StatK<168, 180, 6, Seq<7, 3, 8>, true, 1, Seq<9, 5, 4>, true, 1, true>;
+// single-buffer 12- and 8-CTA shapes at three CTAs/SM (EMAX 10 / 9)
+using K_168x180_c12s = StatK<168, 180, 12, Seq<7, 3, 8>, true, 1, Seq<9, 5, 4>, true, 1, true>;
+using K_168x120_c8s = StatK<168, 120, 8, Seq<7, 3, 8>, true, 1, Seq<5, 3, 8>, true, 1, true>;
 // 65536 = 256 x 256 on a 16-CTA cluster (ComplexF32 precision form)
 using K_256x256_c16 = StatK<256, 256, 16, Seq<16, 16>, true, 2, Seq<16, 16>, true, 2>;
 
 static const StaticFour kStatic[] = {
     //                        9  7  5  3 16  8  4  2
     {CFFT_DT_C128, 168, 180, 12, {0, 1, 0, 1, 0, 1, 0, 0}, {1, 0, 1, 0, 0, 0, 1, 0},
-     (const void*)k_four<double2, CFFT_EMAX, K_168x180_c12>, 0},
+     (const void*)k_four_mb<double2, 10, K_168x180_c12s, 3>, 1},
     {CFFT_DT_C64, 168, 180, 12, {0, 1, 0, 1, 0, 1, 0, 0}, {1, 0, 1, 0, 0, 0, 1, 0},
      (const void*)k_four<float2, CFFT_EMAX, K_168x180_c12>, 0},
     {CFFT_DT_C128, 168, 120, 8, {0, 1, 0, 1, 0, 1, 0, 0}, {0, 0, 1, 1, 0, 1, 0, 0},
-     (const void*)k_four<double2, CFFT_EMAX, K_168x120_c8>, 0},
+     (const void*)k_four_mb<double2, 9, K_168x120_c8s, 3>, 1},
     {CFFT_DT_C64, 168, 120, 8, {0, 1, 0, 1, 0, 1, 0, 0}, {0, 0, 1, 1, 0, 1, 0, 0},
      (const void*)k_four<float2, CFFT_EMAX, K_168x120_c8>, 0},
     {CFFT_DT_C128, 168, 180, 6, {0, 1, 0, 1, 0, 1, 0, 0}, {1, 0, 1, 0, 0, 0, 1, 0},
