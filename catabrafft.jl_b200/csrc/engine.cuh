@@ -734,7 +734,9 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
 
     // Rader epilogue: y[g^-j] = x0 + c[j]; y[0] = x0 + sum(x[1:])
     const int XC = p.XP, L = nx - 1;
-    if (C > 1) cl.sync(); else __syncthreads();   // everyone done reading xs
+    // xs was last read in the prologue (the gather and x0); the exchanges'
+    // cluster barriers since then order those reads before these writes
+    if (C == 1) __syncthreads();
 #pragma unroll 4
     for (int idx = tid; idx < N1 * W; idx += T) {
         const int j1 = K::dW(p, idx), j = idx - j1 * W;
@@ -795,8 +797,10 @@ __device__ __forceinline__ void four_body(const KParams& p, unsigned char* smem)
     TwoLevel t4 = p.t4;
     t4.lo = t4lo;
     t4.hi = t4hi;
+    // no trailing cluster barrier: every path's last access to a peer's
+    // shared memory (an exchange, the Rader scatter) is followed by one, so
+    // no peer touches this CTA's shared memory after it returns
     four_transform<V, EMAX, K>(p, buf, bufC, nullptr, xs, red, twA, twC, t4, t, -1, c);
-    if (C > 1) cl.sync();                 // keep smem alive for peers
 }
 
 // ------------------------------------------------------- COLPASS / ROWPASS
