@@ -35,6 +35,8 @@ FLAG = int
 PLANNER_DEFAULT = NO_FLAG
 
 __all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache", "Batch", "Server",
+           "export_wisdom", "import_wisdom", "forget_wisdom", "wisdom_entries",
+           "rfft", "irfft", "brfft", "plan_rfft", "plan_brfft", "RSpell",
            "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
            "describe_strategy", "version"]
 
@@ -363,10 +365,154 @@ class Server:
             pass
 
 
+# ------------------------------------------------------------ real input
+def _real_code(dt) -> int:
+    name = str(dt).replace("torch.", "")
+    if name in ("float64", "<class 'numpy.float64'>"):
+        return C128
+    if name in ("float32", "<class 'numpy.float32'>"):
+        return C64
+    raise TypeError(f"unsupported real element type {dt}: expected float64 or float32")
+
+
+_rplans = {}
+
+
+class _RPlan:
+    """Owns one cfft_rplan (n reals <-> n/2 + 1 complex, batch transforms)."""
+
+    def __init__(self, n, batch, dtype, flags):
+        h = ctypes.c_void_p()
+        check(_lib.LIB.cfft_rfft_plan_create(ctypes.byref(h), n, batch, dtype, flags))
+        self.handle, self.n, self.batch, self.dtype = h, n, batch, dtype
+
+    def destroy(self):
+        if self.handle:
+            _lib.LIB.cfft_rfft_plan_destroy(self.handle)
+            self.handle = None
+
+
+def _get_rplan(n, batch, dtype, flags, device):
+    key = (device, n, batch, dtype, flags)
+    with _cache_lock:
+        p = _rplans.get(key)
+        if p is None:
+            p = _RPlan(n, batch, dtype, flags)
+            _rplans[key] = p
+        return p
+
+
+def _rrun(x, n, direction, flags=NO_FLAG):
+    """direction FORWARD: reals [.., n] -> complex [.., n//2+1]; else the reverse."""
+    fwd = direction == FORWARD
+    if _is_torch(x) and x.is_cuda:
+        import torch
+        xc = x.contiguous()
+        rows = 1 if xc.dim() == 1 else xc.shape[0]
+        dt = _real_code(xc.dtype) if fwd else _dtype_code(xc.dtype)
+        rdt = torch.float64 if dt == C128 else torch.float32
+        cdt = torch.complex128 if dt == C128 else torch.complex64
+        shp = (n // 2 + 1,) if fwd else (n,)
+        if xc.dim() == 2:
+            shp = (rows,) + shp
+        y = torch.empty(shp, dtype=cdt if fwd else rdt, device=xc.device)
+        plan = _get_rplan(n, rows, dt, flags, xc.device.index)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(xc.device).cuda_stream)
+        with torch.cuda.device(xc.device):
+            if fwd:
+                check(_lib.LIB.cfft_rfft_execute(plan.handle, ctypes.c_void_p(xc.data_ptr()),
+                                                 ctypes.c_void_p(y.data_ptr()), stream))
+            else:
+                check(_lib.LIB.cfft_rfft_execute_inverse(plan.handle, ctypes.c_void_p(xc.data_ptr()),
+                                                         ctypes.c_void_p(y.data_ptr()), direction, stream))
+        return y
+    if _is_torch(x):
+        import torch
+        return torch.from_numpy(_rrun(x.detach().numpy(), n, direction, flags))
+    a = np.ascontiguousarray(np.asarray(x))
+    if a.ndim not in (1, 2):
+        raise ValueError("expected a vector or a [batch, n] matrix")
+    rows = 1 if a.ndim == 1 else a.shape[0]
+    dt = _real_code(a.dtype) if fwd else _dtype_code(a.dtype)
+    if fwd and a.shape[-1] != n:
+        raise ValueError("length mismatch")
+    if not fwd and a.shape[-1] != n // 2 + 1:
+        raise ValueError(f"expected {n // 2 + 1} spectrum values for n = {n}")
+    shp = (n // 2 + 1,) if fwd else (n,)
+    if a.ndim == 2:
+        shp = (rows,) + shp
+    y = np.empty(shp, dtype=(np.complex128 if dt == C128 else np.complex64) if fwd
+                 else (np.float64 if dt == C128 else np.float32))
+    plan = _get_rplan(n, rows, dt, flags, 0)
+    check(_lib.LIB.cfft_rfft_execute_host(plan.handle, a.ctypes.data_as(ctypes.c_void_p),
+                                          y.ctypes.data_as(ctypes.c_void_p), direction))
+    return y
+
+
+def rfft(x):
+    """Real-input forward DFT: n reals -> n//2 + 1 complex (AbstractFFTs.rfft)."""
+    n = x.shape[-1]
+    if n < 1:
+        raise ValueError("transform length must be >= 1")
+    return _rrun(x, n, FORWARD)
+
+
+def irfft(X, n: int):
+    """Inverse of rfft for a Hermitian spectrum of n//2 + 1 values, scaled 1/n."""
+    return _rrun(X, int(n), INVERSE)
+
+
+def brfft(X, n: int):
+    """Unscaled irfft (AbstractFFTs.brfft)."""
+    return _rrun(X, int(n), BACKWARD)
+
+
+class RSpell:
+    """Real-input plan (the reference's plan_rfft / plan_brfft stubs,
+    src/CatabraFFT.jl:199-209): ``p * x`` runs rfft (or, for a plan made by
+    plan_brfft, brfft) with the plan's flag."""
+
+    def __init__(self, n: int, flag: int = NO_FLAG, backward: bool = False):
+        self.n, self.flag, self.backward = int(n), int(flag), backward
+
+    def __mul__(self, x):
+        return _rrun(x, self.n, BACKWARD if self.backward else FORWARD, self.flag)
+
+
+def plan_rfft(x, flag: int = NO_FLAG) -> RSpell:
+    return RSpell(np.asarray(x).shape[-1] if not _is_torch(x) else x.shape[-1], flag)
+
+
+def plan_brfft(X, d: int, flag: int = NO_FLAG) -> RSpell:
+    return RSpell(d, flag, backward=True)
+
+
+def export_wisdom(path) -> None:
+    """Save the shapes MEASURE/ENCHANT chose in this process (spells.jl's
+    serialisable-Spell intent)."""
+    check(_lib.LIB.cfft_wisdom_export(str(path).encode()))
+
+
+def import_wisdom(path) -> None:
+    """Merge a wisdom file: later MEASURE/ENCHANT plans of those keys skip timing."""
+    check(_lib.LIB.cfft_wisdom_import(str(path).encode()))
+
+
+def forget_wisdom() -> None:
+    check(_lib.LIB.cfft_wisdom_forget())
+
+
+def wisdom_entries() -> int:
+    return int(_lib.LIB.cfft_wisdom_entries())
+
+
 def empty_cache() -> None:
     """Free every cached plan and its device memory (CatabraFFT.empty_cache)."""
     with _cache_lock:
         for p in _plans.values():
             p.destroy()
         _plans.clear()
+        for p in _rplans.values():
+            p.destroy()
+        _rplans.clear()
     check(_lib.LIB.cfft_empty_cache())

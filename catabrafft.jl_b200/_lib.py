@@ -46,6 +46,15 @@ SIGNATURES = {
     "cfft_serve_drain": (_ci, [_vp]),
     "cfft_serve_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "cfft_serve_destroy": (_ci, [_vp]),
+    "cfft_rfft_plan_create": (_ci, [ctypes.POINTER(_vp), _i64, _i64, _ci, _ci]),
+    "cfft_rfft_execute": (_ci, [_vp, _vp, _vp, _vp]),
+    "cfft_rfft_execute_inverse": (_ci, [_vp, _vp, _vp, _ci, _vp]),
+    "cfft_rfft_execute_host": (_ci, [_vp, _vp, _vp, _ci]),
+    "cfft_rfft_plan_destroy": (_ci, [_vp]),
+    "cfft_wisdom_export": (_ci, [_cp]),
+    "cfft_wisdom_import": (_ci, [_cp]),
+    "cfft_wisdom_forget": (_ci, []),
+    "cfft_wisdom_entries": (_i64, []),
 }
 
 

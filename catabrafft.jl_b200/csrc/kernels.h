@@ -31,5 +31,15 @@ cudaError_t cfft_gen_bluestein_b(double2* b, const double2* ch, long long n, lon
 cudaError_t cfft_gen_rader_b(double2* b, const int* iperm, long long n, long long M, int exact,
                              double2 winv, cudaStream_t st);
 cudaError_t cfft_scale(double2* v, long long M, double s, cudaStream_t st);
+// real-input transforms (real.cu)
+cudaError_t cfft_r2c_post(void* out, long long N, long long n, long long batch, long long dist, int dtype,
+                          cudaStream_t st);
+cudaError_t cfft_c2r_pre(const void* in, void* z, long long N, long long n, long long batch, long long in_dist,
+                         double scale, int dtype, cudaStream_t st);
+cudaError_t cfft_r2c_widen(const void* x, void* s, long long n, long long batch, int dtype, cudaStream_t st);
+cudaError_t cfft_r2c_keep(const void* s, void* out, long long n, long long batch, int dtype, cudaStream_t st);
+cudaError_t cfft_c2r_expand(const void* in, void* s, long long n, long long batch, double scale, int dtype,
+                            cudaStream_t st);
+cudaError_t cfft_c2r_real(const void* s, void* x, long long n, long long batch, int dtype, cudaStream_t st);
 // set the thread-local text returned by cfft_last_error() (fixed buffer)
 void cfft_set_last_error(const char* msg);

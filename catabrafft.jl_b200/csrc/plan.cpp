@@ -606,7 +606,7 @@ static int make_twolevel(cfft_plan_s* P, int64_t N, TwoLevel& t) {
 
 static int plan_build(cfft_plan_s* P, const Shape& sh);
 static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cudaStream_t st,
-                        int64_t nbatch = -1);
+                        int64_t nbatch = -1, int64_t in_dist = -1, int64_t out_dist = -1);
 static void plan_free(cfft_plan_s* P);
 
 static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dtype, int flags);
@@ -934,12 +934,15 @@ static void plan_free(cfft_plan_s* P) {
     P->scratch[0] = P->scratch[1] = nullptr;
 }
 
+// in_dist / out_dist: elements between consecutive transforms of the caller's
+// input and output (default n)
 static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cudaStream_t st,
-                        int64_t nbatch) {
+                        int64_t nbatch, int64_t in_dist, int64_t out_dist) {
     if (dir < 0 || dir > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
     const size_t e = elem_bytes(P->dtype);
     const int64_t n = P->n;
     const int64_t total = (nbatch < 0) ? P->batch : std::min(nbatch, P->batch);
+    const int64_t idist = in_dist < 0 ? n : in_dist, odist = out_dist < 0 ? n : out_dist;
     if (((uintptr_t)in % e) != 0 || ((uintptr_t)out % e) != 0)
         return fail(CFFT_ERR_INVALID, "buffers must be aligned to the element size");
     for (int64_t b0 = 0; b0 < total; b0 += P->chunk) {
@@ -949,15 +952,16 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             kp.dir = dir;
             kp.scale = (dir == CFFT_INVERSE) ? 1.0 / (double)n : 1.0;
             kp.batch = (int)nb;
-            const char* user_in = (const char*)in + (size_t)b0 * n * e;
-            char* user_out = (char*)out + (size_t)b0 * n * e;
+            const char* user_in = (const char*)in + (size_t)b0 * idist * e;
+            char* user_out = (char*)out + (size_t)b0 * odist * e;
             auto sel = [&](int w) -> void* {
                 return w == 0 ? (void*)user_in : w == 1 ? (void*)user_out : P->scratch[w - 2];
             };
             kp.in = sel(s.in_sel);
             kp.out = sel(s.out_sel);
-            kp.in_dist = (s.in_sel >= 2) ? P->shape.M : n;
-            kp.out_dist = (s.out_sel >= 2) ? P->shape.M : n;
+            auto dist = [&](int sel) -> int64_t { return sel >= 2 ? P->shape.M : sel == 0 ? idist : odist; };
+            kp.in_dist = dist(s.in_sel);
+            kp.out_dist = dist(s.out_sel);
             unsigned grid;
             if (kp.mode == MODE_ROWS) grid = (unsigned)((nb + kp.V - 1) / kp.V);
             else if (kp.mode == MODE_FOUR) grid = (unsigned)(nb * kp.C);
@@ -990,6 +994,43 @@ static float time_plan(cfft_plan_s* P, void* buf) {
     return ms / reps;
 }
 
+// ------------------------------------------------------------------ wisdom
+// Shapes chosen by MEASURE / ENCHANT, keyed by (n, batch, dtype, flags), so
+// a later process can skip the timing: the reference's intent for its
+// serialisable Spell (src/spells.jl:180-375, left unfinished there).  An
+// entry names a shape by its signature; on use it must still be one of the
+// planner's candidates for that key, else the planner times as usual.
+struct WisdomKey {
+    int64_t n, batch;
+    int dtype, flags;
+    bool operator<(const WisdomKey& o) const {
+        return std::tie(n, batch, dtype, flags) < std::tie(o.n, o.batch, o.dtype, o.flags);
+    }
+};
+static std::mutex g_wis_mu;
+static std::map<WisdomKey, std::string> g_wisdom;
+
+static std::string shape_signature(const Shape& s) {
+    std::string r = std::to_string(s.mode) + " " + std::to_string(s.conv) + " " + std::to_string(s.M) + " " +
+                    std::to_string(s.N1) + " " + std::to_string(s.N2) + " " + std::to_string(s.C) + " " +
+                    std::to_string(s.V) + " a";
+    for (int x : s.ra) r += " " + std::to_string(x);
+    r += " c";
+    for (int x : s.rc) r += " " + std::to_string(x);
+    return r;
+}
+static bool wisdom_lookup(const WisdomKey& k, std::string& sig) {
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    auto it = g_wisdom.find(k);
+    if (it == g_wisdom.end()) return false;
+    sig = it->second;
+    return true;
+}
+static void wisdom_store(const WisdomKey& k, const std::string& sig) {
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    g_wisdom[k] = sig;
+}
+
 static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dtype, int flags) {
     if (!out) return fail(CFFT_ERR_INVALID, "plan pointer is null");
     if (n < 1 || batch < 1) return fail(CFFT_ERR_INVALID, "n and batch must be >= 1");
@@ -1013,6 +1054,20 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
             plan_free(P);
         }
     } else {
+        const WisdomKey wk{n, batch, dtype, flags};
+        std::string sig;
+        if (wisdom_lookup(wk, sig)) {
+            for (auto& c : cands) {
+                if (shape_signature(c) != sig) continue;
+                rc = plan_build(P, c);
+                if (rc == CFFT_OK) {
+                    *out = P;
+                    return CFFT_OK;
+                }
+                plan_free(P);
+                break;
+            }
+        }
         // MEASURE: the best few heuristic candidates; ENCHANT: all of them
         size_t limit = (level == CFFT_MEASURE) ? std::min<size_t>(cands.size(), 4) : cands.size();
         limit = std::min<size_t>(limit, 24);
@@ -1043,6 +1098,7 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
         cudaFree(buf);
         if (best_i < 0) { delete P; return fail(CFFT_ERR_UNSUPPORTED, "no candidate plan ran"); }
         rc = plan_build(P, cands[best_i]);
+        if (rc == CFFT_OK) wisdom_store(wk, shape_signature(cands[best_i]));
     }
     if (rc != CFFT_OK) {
         std::string keep = g_err;
@@ -2100,5 +2156,190 @@ int cfft_serve_destroy(cfft_server server) {
     if (!server) return fail(CFFT_ERR_INVALID, "null server");
     serve_free(server);
     delete server;
+    return CFFT_OK;
+}
+
+// Wisdom file: a header line, then one line per entry:
+//   n batch dtype flags | mode conv M N1 N2 C V a <radices> c <radices>
+int cfft_wisdom_export(const char* path) {
+    if (!path) return fail(CFFT_ERR_INVALID, "null path");
+    FILE* f = fopen(path, "w");
+    if (!f) return fail(CFFT_ERR_INVALID, std::string("cannot write ") + path);
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    fprintf(f, "catabra-b200-wisdom 1\n");
+    for (auto& kv : g_wisdom)
+        fprintf(f, "%lld %lld %d %d | %s\n", (long long)kv.first.n, (long long)kv.first.batch, kv.first.dtype,
+                kv.first.flags, kv.second.c_str());
+    const bool bad = ferror(f) != 0;
+    fclose(f);
+    return bad ? fail(CFFT_ERR_INVALID, std::string("write failed: ") + path) : CFFT_OK;
+}
+
+int cfft_wisdom_import(const char* path) {
+    if (!path) return fail(CFFT_ERR_INVALID, "null path");
+    FILE* f = fopen(path, "r");
+    if (!f) return fail(CFFT_ERR_INVALID, std::string("cannot read ") + path);
+    char line[1024];
+    std::map<WisdomKey, std::string> got;
+    int rc = CFFT_OK;
+    if (!fgets(line, sizeof line, f) || strncmp(line, "catabra-b200-wisdom 1", 21) != 0) {
+        rc = fail(CFFT_ERR_INVALID, "not a wisdom file (missing header)");
+    } else {
+        while (fgets(line, sizeof line, f)) {
+            long long n = 0, b = 0;
+            int dt = 0, fl = 0, used = 0;
+            if (line[0] == '\n' || line[0] == '#') continue;
+            if (sscanf(line, "%lld %lld %d %d | %n", &n, &b, &dt, &fl, &used) != 4 || used == 0 || n < 1 || b < 1 ||
+                (dt != CFFT_C128 && dt != CFFT_C64)) {
+                rc = fail(CFFT_ERR_INVALID, std::string("malformed wisdom line: ") + line);
+                break;
+            }
+            std::string sig(line + used);
+            while (!sig.empty() && (sig.back() == '\n' || sig.back() == '\r' || sig.back() == ' ')) sig.pop_back();
+            got[WisdomKey{n, b, dt, fl}] = sig;
+        }
+    }
+    fclose(f);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    for (auto& kv : got) g_wisdom[kv.first] = kv.second;
+    return CFFT_OK;
+}
+
+int cfft_wisdom_forget(void) {
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    g_wisdom.clear();
+    return CFFT_OK;
+}
+
+int64_t cfft_wisdom_entries(void) {
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    return (int64_t)g_wisdom.size();
+}
+
+// ------------------------------------------------------------ real input
+// rfft / irfft / brfft (AbstractFFTs' plan_rfft / plan_brfft, stubs in the
+// reference at src/CatabraFFT.jl:199-209).  Even n runs a complex FFT of n/2
+// points on the reals read as complex pairs plus one post- (pre-) processing
+// kernel; odd n goes through the complex path of n points on a scratch.
+struct cfft_rplan_s {
+    int64_t n = 0, batch = 0;
+    int dtype = 0;
+    cfft_plan_s* P = nullptr;
+    void* scratch = nullptr;     // odd n: batch * n complex
+    void* d_real = nullptr;      // host entry: device copies of the two sides
+    void* d_cplx = nullptr;
+    std::mutex mu;
+};
+
+int cfft_rfft_plan_create(cfft_rplan* plan, int64_t n, int64_t batch, int dtype, int flags) {
+    g_err[0] = 0;
+    if (!plan) return fail(CFFT_ERR_INVALID, "plan pointer is null");
+    *plan = nullptr;
+    if (n < 1 || batch < 1) return fail(CFFT_ERR_INVALID, "n and batch must be >= 1");
+    if (dtype != CFFT_C128 && dtype != CFFT_C64) return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128 or CFFT_C64");
+    cfft_rplan_s* R = new cfft_rplan_s();
+    R->n = n;
+    R->batch = batch;
+    R->dtype = dtype;
+    const bool even = (n % 2 == 0);
+    int rc = plan_create_impl(&R->P, even ? n / 2 : n, batch, dtype, flags);
+    if (rc == CFFT_OK && !even) {
+        if (cudaMalloc(&R->scratch, (size_t)n * batch * elem_bytes(dtype)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(CFFT_ERR_NOMEM, "real-transform scratch allocation failed");
+        }
+    }
+    if (rc) {
+        std::string keep = g_err;
+        if (R->P) {
+            plan_free(R->P);
+            delete R->P;
+        }
+        delete R;
+        cfft_set_last_error(keep.c_str());
+        return rc;
+    }
+    *plan = R;
+    return CFFT_OK;
+}
+
+int cfft_rfft_execute(cfft_rplan plan, const void* d_real, void* d_complex, void* stream) {
+    if (!plan || !d_real || !d_complex) return fail(CFFT_ERR_INVALID, "null plan or buffer");
+    cfft_rplan_s* R = plan;
+    const size_t e = elem_bytes(R->dtype);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = R->n, h = n / 2 + 1;
+    if (n % 2 == 0) {
+        if (((uintptr_t)d_real % e) != 0 || ((uintptr_t)d_complex % e) != 0)
+            return fail(CFFT_ERR_INVALID, "buffers must be aligned to the complex element size");
+        int rc = plan_execute(R->P, d_real, d_complex, CFFT_FORWARD, st, -1, n / 2, h);
+        if (rc) return rc;
+        CUDA_TRY(cfft_r2c_post(d_complex, n / 2, n, R->batch, h, R->dtype, st));
+        return CFFT_OK;
+    }
+    CUDA_TRY(cfft_r2c_widen(d_real, R->scratch, n, R->batch, R->dtype, st));
+    int rc = plan_execute(R->P, R->scratch, R->scratch, CFFT_FORWARD, st, -1);
+    if (rc) return rc;
+    CUDA_TRY(cfft_r2c_keep(R->scratch, d_complex, n, R->batch, R->dtype, st));
+    return CFFT_OK;
+}
+
+int cfft_rfft_execute_inverse(cfft_rplan plan, const void* d_complex, void* d_real, int direction, void* stream) {
+    if (!plan || !d_real || !d_complex) return fail(CFFT_ERR_INVALID, "null plan or buffer");
+    if (direction != CFFT_INVERSE && direction != CFFT_BACKWARD)
+        return fail(CFFT_ERR_INVALID, "direction must be CFFT_INVERSE (irfft) or CFFT_BACKWARD (brfft)");
+    cfft_rplan_s* R = plan;
+    const size_t e = elem_bytes(R->dtype);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = R->n, h = n / 2 + 1;
+    const double scale = (direction == CFFT_INVERSE) ? 1.0 / (double)n : 1.0;
+    if (n % 2 == 0) {
+        if (((uintptr_t)d_real % e) != 0 || ((uintptr_t)d_complex % e) != 0)
+            return fail(CFFT_ERR_INVALID, "buffers must be aligned to the complex element size");
+        CUDA_TRY(cfft_c2r_pre(d_complex, d_real, n / 2, n, R->batch, h, scale, R->dtype, st));
+        return plan_execute(R->P, d_real, d_real, CFFT_BACKWARD, st, -1);
+    }
+    CUDA_TRY(cfft_c2r_expand(d_complex, R->scratch, n, R->batch, scale, R->dtype, st));
+    int rc = plan_execute(R->P, R->scratch, R->scratch, CFFT_BACKWARD, st, -1);
+    if (rc) return rc;
+    CUDA_TRY(cfft_c2r_real(R->scratch, d_real, n, R->batch, R->dtype, st));
+    return CFFT_OK;
+}
+
+int cfft_rfft_execute_host(cfft_rplan plan, const void* h_in, void* h_out, int direction) {
+    if (!plan || !h_in || !h_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
+    if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    cfft_rplan_s* R = plan;
+    std::lock_guard<std::mutex> lk(R->mu);
+    const size_t e = elem_bytes(R->dtype);
+    const size_t rbytes = (size_t)R->n * R->batch * (e / 2), cbytes = (size_t)(R->n / 2 + 1) * R->batch * e;
+    if (!R->d_real) {
+        CUDA_TRY(cudaMalloc(&R->d_real, rbytes + e));
+        CUDA_TRY(cudaMalloc(&R->d_cplx, cbytes));
+    }
+    int rc;
+    if (direction == CFFT_FORWARD) {
+        CUDA_TRY(cudaMemcpy(R->d_real, h_in, rbytes, cudaMemcpyHostToDevice));
+        rc = cfft_rfft_execute(R, R->d_real, R->d_cplx, nullptr);
+        if (rc == CFFT_OK) CUDA_TRY(cudaMemcpy(h_out, R->d_cplx, cbytes, cudaMemcpyDeviceToHost));
+    } else {
+        CUDA_TRY(cudaMemcpy(R->d_cplx, h_in, cbytes, cudaMemcpyHostToDevice));
+        rc = cfft_rfft_execute_inverse(R, R->d_cplx, R->d_real, direction, nullptr);
+        if (rc == CFFT_OK) CUDA_TRY(cudaMemcpy(h_out, R->d_real, rbytes, cudaMemcpyDeviceToHost));
+    }
+    return rc;
+}
+
+int cfft_rfft_plan_destroy(cfft_rplan plan) {
+    if (!plan) return fail(CFFT_ERR_INVALID, "null plan");
+    if (plan->d_real) cudaFree(plan->d_real);
+    if (plan->d_cplx) cudaFree(plan->d_cplx);
+    if (plan->P) {
+        plan_free(plan->P);
+        delete plan->P;
+    }
+    if (plan->scratch) cudaFree(plan->scratch);
+    delete plan;
     return CFFT_OK;
 }

@@ -118,6 +118,38 @@ int cfft_batch_destroy(cfft_batch batch);
 int64_t cfft_batch_elements(cfft_batch batch);
 int cfft_batch_launches(cfft_batch batch);
 
+/* Real-input transforms: plan_rfft / plan_brfft (src/CatabraFFT.jl:199-209,
+ * stubs in the reference) with AbstractFFTs semantics.  A plan covers
+ * `batch` transforms of n reals (CFFT_C128: double, CFFT_C64: float) and
+ * their n/2 + 1 complex spectra, both packed back to back.
+ *   cfft_rfft_execute          n reals -> n/2 + 1 complex (rfft)
+ *   cfft_rfft_execute_inverse  n/2 + 1 complex -> n reals, CFFT_INVERSE =
+ *                              irfft (scaled 1/n), CFFT_BACKWARD = brfft; the
+ *                              imaginary parts of X[0] (and X[n/2], n even)
+ *                              are ignored.  The complex input is not modified.
+ * Buffers must be aligned to the complex element size (16 / 8 bytes). */
+typedef struct cfft_rplan_s* cfft_rplan;
+int cfft_rfft_plan_create(cfft_rplan* plan, int64_t n, int64_t batch, int dtype, int flags);
+int cfft_rfft_execute(cfft_rplan plan, const void* d_real, void* d_complex, void* stream);
+int cfft_rfft_execute_inverse(cfft_rplan plan, const void* d_complex, void* d_real, int direction, void* stream);
+/* Host-buffer form (the ccall path): direction CFFT_FORWARD takes n reals
+ * per transform and returns n/2 + 1 complex; CFFT_INVERSE / CFFT_BACKWARD the
+ * reverse.  Copies in, transforms, copies out, synchronises. */
+int cfft_rfft_execute_host(cfft_rplan plan, const void* h_in, void* h_out, int direction);
+int cfft_rfft_plan_destroy(cfft_rplan plan);
+
+/* Wisdom: the shapes MEASURE / ENCHANT chose, saved across processes --
+ * the reference meant its Spell to be serialisable (src/spells.jl:180-375,
+ * never finished).  A plan created with MEASURE or ENCHANT whose key
+ * (n, batch, dtype, flags) has wisdom builds that shape without timing, as
+ * long as it is still one of the planner's candidates.  Export writes every
+ * entry of this process; import merges a file's entries (a bad file changes
+ * nothing and returns CFFT_ERR_INVALID); forget drops them all. */
+int cfft_wisdom_export(const char* path);
+int cfft_wisdom_import(const char* path);
+int cfft_wisdom_forget(void);
+int64_t cfft_wisdom_entries(void);
+
 /* Serving form: requests of any length arrive one at a time, from any host
  * thread, with device buffers; the reference runs each call to completion on
  * the calling thread (fft/ifft/bfft, src/CatabraFFT.jl:65-115).

@@ -55,6 +55,12 @@ def test_invalid_arguments_return_status():
     assert lib.cfft_serve_drain(None) == m._lib.ERR_INVALID
     assert lib.cfft_serve_destroy(None) == m._lib.ERR_INVALID
     assert lib.cfft_batch_create(None, 1, None, 0, 0) == m._lib.ERR_INVALID
+    rp = ctypes.c_void_p()
+    assert lib.cfft_rfft_plan_create(None, 16, 1, 0, 0) == m._lib.ERR_INVALID
+    assert lib.cfft_rfft_plan_create(ctypes.byref(rp), 0, 1, 0, 0) == m._lib.ERR_INVALID
+    assert lib.cfft_rfft_plan_create(ctypes.byref(rp), 16, 1, 9, 0) == m._lib.ERR_INVALID
+    assert lib.cfft_rfft_execute(None, None, None, None) == m._lib.ERR_INVALID
+    assert lib.cfft_rfft_plan_destroy(None) == m._lib.ERR_INVALID
 
 
 def test_python_api_argument_errors():
