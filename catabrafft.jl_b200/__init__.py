@@ -28,7 +28,7 @@ import threading
 import numpy as np
 
 from . import _lib
-from ._lib import (BACKWARD, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERSE, MEASURE,
+from ._lib import (BACKWARD, C32, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERSE, MEASURE,
                    NO_FLAG, SERVE_BATCHED, SERVE_DIRECT, CatabraError, check)
 
 FLAG = int
@@ -36,7 +36,8 @@ PLANNER_DEFAULT = NO_FLAG
 
 __all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache", "Batch", "Server",
            "export_wisdom", "import_wisdom", "forget_wisdom", "wisdom_entries",
-           "rfft", "irfft", "brfft", "plan_rfft", "plan_brfft", "RSpell",
+           "rfft", "irfft", "brfft", "plan_rfft", "plan_brfft", "RSpell", "plan_bfft", "plan_ifft",
+           "plan_inv",
            "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
            "describe_strategy", "version"]
 
@@ -61,6 +62,8 @@ def _dtype_code(dt) -> int:
         return C128
     if name in ("complex64", "<class 'numpy.complex64'>"):
         return C64
+    if name in ("complex32", "chalf"):        # torch.complex32: ComplexF16
+        return C32
     raise TypeError(f"unsupported element type {dt}: expected complex128 or complex64")
 
 
@@ -192,13 +195,16 @@ class Spell:
     NO_FLAG function) and x is never overwritten.
     """
 
-    def __init__(self, n: int, datatype, flag: int = NO_FLAG, batch: int = 1, device: int = 0):
+    def __init__(self, n: int, datatype, flag: int = NO_FLAG, batch: int = 1, device: int = 0,
+                 direction: int = FORWARD):
         if n < 1:
             raise ValueError("transform length must be >= 1")
         self.n = int(n)
         self.datatype = datatype
         self.flag = int(flag)
         self.batch = int(batch)
+        self.device = device
+        self.direction = int(direction)
         self.inverse = None
         self._plan = _get_plan(self.n, self.batch, _dtype_code(datatype), self.flag, device)
 
@@ -215,15 +221,64 @@ class Spell:
 
     def __mul__(self, x):
         self._check(x)
-        return _run(x, FORWARD, self.flag)
+        return _run(x, self.direction, self.flag)
 
     __matmul__ = __mul__
 
     def __call__(self, x):
-        return fft(x)
+        return self * x
+
+    def adjoint(self) -> "Spell":
+        """The adjoint (AbstractFFTs.adjoint_mul, CatabraFFT.jl:214-219): the
+        DFT of the opposite sign with the same scaling -- bfft for a forward
+        plan, fft for a bfft plan, fft / n for an ifft plan."""
+        if self.direction == FORWARD:
+            return Spell(self.n, self.datatype, self.flag, self.batch, self.device, BACKWARD)
+        if self.direction == BACKWARD:
+            return Spell(self.n, self.datatype, self.flag, self.batch, self.device, FORWARD)
+        return _ScaledSpell(self, 1.0 / self.n)
 
     def __repr__(self):
-        return f"Spell{{{self.datatype}}}(n={self.n}, flag={self.flag}, batch={self.batch})"
+        kind = {FORWARD: "fft", INVERSE: "ifft", BACKWARD: "bfft"}[self.direction]
+        return f"Spell{{{self.datatype}}}({kind}, n={self.n}, flag={self.flag}, batch={self.batch})"
+
+
+class _ScaledSpell:
+    """c * fft: the adjoint of an ifft plan."""
+
+    def __init__(self, p: Spell, c: float):
+        self.p, self.c = p, c
+
+    def __mul__(self, x):
+        self.p._check(x)
+        return _run(x, FORWARD, self.p.flag) * self.c
+
+
+def plan_inv(p: Spell) -> Spell:
+    """Inverse plan, cached on p (AbstractFFTs.plan_inv; the reference's
+    CatabraFFT.jl:181-184): ifft for a forward plan, fft for an ifft plan,
+    fft / n for a bfft plan."""
+    if p.inverse is None:
+        if p.direction == FORWARD:
+            p.inverse = Spell(p.n, p.datatype, p.flag, p.batch, p.device, INVERSE)
+        elif p.direction == INVERSE:
+            p.inverse = Spell(p.n, p.datatype, p.flag, p.batch, p.device, FORWARD)
+        else:
+            p.inverse = _ScaledSpell(Spell(p.n, p.datatype, p.flag, p.batch, p.device, FORWARD), 1.0 / p.n)
+    return p.inverse
+
+
+def plan_bfft(x, flags: int = NO_FLAG) -> Spell:
+    """Plan an unnormalised backward FFT (AbstractFFTs.plan_bfft; a stub in
+    the reference, CatabraFFT.jl:173-177)."""
+    n, batch = _shape(x)
+    return Spell(n, x.dtype, flags, batch, _current_device(x), BACKWARD)
+
+
+def plan_ifft(x, flags: int = NO_FLAG) -> Spell:
+    """Plan an inverse FFT scaled by 1/n (AbstractFFTs.plan_ifft)."""
+    n, batch = _shape(x)
+    return Spell(n, x.dtype, flags, batch, _current_device(x), INVERSE)
 
 
 def plan_fft(x, flags: int = NO_FLAG) -> Spell:

@@ -11,7 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcatabra_b200.so")
 
-C128, C64 = 0, 1
+C128, C64, C32 = 0, 1, 2
 FORWARD, INVERSE, BACKWARD = 0, 1, 2
 NO_FLAG, MEASURE, ENCHANT, EXACT_TWIDDLES = 0, 1, 2, 16
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED = 0, 1, 2, 3, 4

@@ -41,5 +41,8 @@ cudaError_t cfft_r2c_keep(const void* s, void* out, long long n, long long batch
 cudaError_t cfft_c2r_expand(const void* in, void* s, long long n, long long batch, double scale, int dtype,
                             cudaStream_t st);
 cudaError_t cfft_c2r_real(const void* s, void* x, long long n, long long batch, int dtype, cudaStream_t st);
+// ComplexF16 <-> ComplexF32 element conversion (real.cu)
+cudaError_t cfft_half_to_float(const void* in, void* out, long long count, cudaStream_t st);
+cudaError_t cfft_float_to_half(const void* in, void* out, long long count, cudaStream_t st);
 // set the thread-local text returned by cfft_last_error() (fixed buffer)
 void cfft_set_last_error(const char* msg);

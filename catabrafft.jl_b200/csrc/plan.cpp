@@ -275,6 +275,10 @@ struct cfft_plan_s {
     void* host_buf[3] = {nullptr, nullptr, nullptr};
     cudaStream_t host_st[3] = {nullptr, nullptr, nullptr};   // in, compute, out
     cudaEvent_t ev_in[3], ev_comp[3], ev_out[3];
+    // ComplexF16 plans: ComplexF16 in/out around the ComplexF32 path
+    bool io_half = false;
+    void* half_work = nullptr;   // batch * n ComplexF32
+    void* half_dev = nullptr;    // host entry: device copy of the ComplexF16 data
 };
 
 static size_t elem_bytes(int dtype) { return dtype == CFFT_C128 ? 16 : 8; }
@@ -1033,8 +1037,28 @@ static void wisdom_store(const WisdomKey& k, const std::string& sig) {
 
 static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dtype, int flags) {
     if (!out) return fail(CFFT_ERR_INVALID, "plan pointer is null");
+    if (dtype == CFFT_C32) {
+        // ComplexF16 data, ComplexF32 arithmetic: a ComplexF32 plan plus one
+        // working buffer the data is widened into and narrowed out of
+        if (n < 1 || batch < 1) return fail(CFFT_ERR_INVALID, "n and batch must be >= 1");
+        int rc = plan_create_impl(out, n, batch, CFFT_C64, flags);
+        if (rc) return rc;
+        cfft_plan_s* P = *out;
+        P->io_half = true;
+        P->desc = "f16io+" + P->desc;
+        if (cudaMalloc(&P->half_work, (size_t)n * batch * sizeof(float2)) != cudaSuccess) {
+            cudaGetLastError();
+            plan_free(P);
+            delete P;
+            *out = nullptr;
+            return fail(CFFT_ERR_NOMEM, "ComplexF16 working buffer allocation failed");
+        }
+        P->allocs.push_back(P->half_work);
+        return CFFT_OK;
+    }
     if (n < 1 || batch < 1) return fail(CFFT_ERR_INVALID, "n and batch must be >= 1");
-    if (dtype != CFFT_C128 && dtype != CFFT_C64) return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128 or CFFT_C64");
+    if (dtype != CFFT_C128 && dtype != CFFT_C64)
+        return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128, CFFT_C64 or CFFT_C32");
     if (n > (1LL << 26)) return fail(CFFT_ERR_UNSUPPORTED, "n above 2^26 is not supported");
     int level = flags & 3;
     if (level > 2) return fail(CFFT_ERR_INVALID, "flag must be NO_FLAG, MEASURE or ENCHANT");
@@ -1812,8 +1836,21 @@ int cfft_plan_create(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int f
     return plan_create_impl(plan, n, batch, dtype, flags);
 }
 
+static int execute_half(cfft_plan_s* P, const void* d_in, void* d_out, int direction, cudaStream_t st) {
+    if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    if (((uintptr_t)d_in % 4) != 0 || ((uintptr_t)d_out % 4) != 0)
+        return fail(CFFT_ERR_INVALID, "ComplexF16 buffers must be 4-byte aligned");
+    const long long count = (long long)P->n * P->batch;
+    CUDA_TRY(cfft_half_to_float(d_in, P->half_work, count, st));
+    int rc = plan_execute(P, P->half_work, P->half_work, direction, st);
+    if (rc) return rc;
+    CUDA_TRY(cfft_float_to_half(P->half_work, d_out, count, st));
+    return CFFT_OK;
+}
+
 int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, void* stream) {
     if (!plan || !d_in || !d_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
+    if (plan->io_half) return execute_half(plan, d_in, d_out, direction, (cudaStream_t)stream);
     return plan_execute(plan, d_in, d_out, direction, (cudaStream_t)stream);
 }
 
@@ -1822,6 +1859,18 @@ int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int directi
     if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
     cfft_plan_s* P = plan;
     std::lock_guard<std::mutex> lk(P->host_mu);
+    if (P->io_half) {
+        const size_t bytes = (size_t)P->n * P->batch * 4;
+        if (!P->half_dev) {
+            CUDA_TRY(cudaMalloc(&P->half_dev, bytes));
+            P->allocs.push_back(P->half_dev);
+        }
+        CUDA_TRY(cudaMemcpy(P->half_dev, h_in, bytes, cudaMemcpyHostToDevice));
+        int rc = execute_half(P, P->half_dev, P->half_dev, direction, nullptr);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpy(h_out, P->half_dev, bytes, cudaMemcpyDeviceToHost));
+        return CFFT_OK;
+    }
     const size_t e = elem_bytes(P->dtype);
     const size_t tbytes = (size_t)P->n * e;
     if (!P->host_ready) {

@@ -15,6 +15,7 @@
 // by the complex path, and the first n/2 + 1 outputs kept; the inverse
 // rebuilds the full Hermitian spectrum there.  Twiddles are evaluated in
 // FP64 (sincospi) and rounded once to the data type.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "engine.cuh"
@@ -147,5 +148,25 @@ cudaError_t cfft_c2r_expand(const void* in, void* s, long long n, long long batc
 cudaError_t cfft_c2r_real(const void* s, void* x, long long n, long long batch, int dtype, cudaStream_t st) {
     if (dtype == CFFT_DT_C128) k_c2r_real<double2, double><<<grid_for(n * batch), 256, 0, st>>>((const double2*)s, (double*)x, n, batch);
     else k_c2r_real<float2, float><<<grid_for(n * batch), 256, 0, st>>>((const float2*)s, (float*)x, n, batch);
+    return cudaGetLastError();
+}
+
+// ComplexF16 input/output around the ComplexF32 path (FP32 arithmetic)
+__global__ void k_h2f(const __half2* in, float2* out, long long count) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = __half22float2(in[i]);
+}
+__global__ void k_f2h(const float2* in, __half2* out, long long count) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = __float22half2_rn(in[i]);
+}
+cudaError_t cfft_half_to_float(const void* in, void* out, long long count, cudaStream_t st) {
+    k_h2f<<<grid_for(count), 256, 0, st>>>((const __half2*)in, (float2*)out, count);
+    return cudaGetLastError();
+}
+cudaError_t cfft_float_to_half(const void* in, void* out, long long count, cudaStream_t st) {
+    k_f2h<<<grid_for(count), 256, 0, st>>>((const float2*)in, (__half2*)out, count);
     return cudaGetLastError();
 }

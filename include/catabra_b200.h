@@ -26,8 +26,12 @@
 extern "C" {
 #endif
 
-/* element types: the reference's Complex{T}, T in {Float64, Float32} */
-enum { CFFT_C128 = 0, CFFT_C64 = 1 };
+/* element types: the reference's Complex{T}, T in {Float64, Float32} and
+ * Float16 (ComplexF16, which the reference's self-test uses,
+ * test/runtests.jl:39): ComplexF16 data is transformed with FP32 arithmetic
+ * and rounded once on output; plans, execution, cfft_fft and the host entry
+ * accept it (the batched, serving and real-input forms do not). */
+enum { CFFT_C128 = 0, CFFT_C64 = 1, CFFT_C32 = 2 };
 
 /* directions: fft (CatabraFFT.jl:65-72), ifft with 1/n (:88-101),
  * bfft without scaling (:103-115) */

@@ -73,3 +73,50 @@ def test_rfft_invalid_direction(cb):
     buf = ctypes.c_void_p(1 << 20)
     assert lib.cfft_rfft_execute_inverse(h, buf, buf, cb.FORWARD, None) == cb._lib.ERR_INVALID
     lib.cfft_rfft_plan_destroy(h)
+
+
+def test_plan_inverse_bfft_adjoint(cb):
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((2, 30240)) + 1j * rng.standard_normal((2, 30240))
+    p = cb.plan_fft(x)
+    X = p * x
+    assert rel(X, np.fft.fft(x, axis=1)) < 1e-12
+    assert rel(cb.plan_inv(p) * X, x) < 2e-12
+    assert cb.plan_inv(p) is cb.plan_inv(p)
+    pb = cb.plan_bfft(x)
+    assert rel(pb * X, 30240 * x) < 2e-12
+    assert rel(cb.plan_inv(pb) * (30240 * x), X) < 2e-12
+    pi = cb.plan_ifft(x)
+    assert rel(pi * X, x) < 2e-12
+    # adjoints: <p x, y> = <x, p' y>
+    y = rng.standard_normal((2, 30240)) + 1j * rng.standard_normal((2, 30240))
+    for q in (p, pb, pi):
+        lhs = np.vdot(q * x, y)
+        rhs = np.vdot(x, q.adjoint() * y)
+        assert abs(lhs - rhs) / abs(lhs) < 1e-11
+
+
+def test_complex_f16(cb):
+    """ComplexF16 data (the reference's self-test type), FP32 arithmetic."""
+    import ctypes
+    import torch
+    import oracle
+    n, batch = 4096, 3
+    x32 = torch.randn(batch, n, dtype=torch.complex64, device="cuda")
+    xh = x32.to(torch.complex32)
+    y = cb.fft(xh)
+    assert y.dtype == torch.complex32
+    ref = oracle.fft(xh.to(torch.complex128).cpu().numpy())
+    assert rel(y.to(torch.complex128).cpu().numpy(), ref) < 2e-3
+    # host entry: interleaved float16 pairs
+    lib = cb._lib.LIB
+    h = ctypes.c_void_p()
+    cb.check(lib.cfft_plan_create(ctypes.byref(h), n, batch, cb.C32, 0))
+    hin = xh.cpu().view(torch.float16).numpy().copy()
+    hout = np.empty_like(hin)
+    cb.check(lib.cfft_execute_host(h, hin.ctypes.data_as(ctypes.c_void_p), hout.ctypes.data_as(ctypes.c_void_p), 1))
+    back = hout.astype(np.float64).reshape(batch, n, 2)
+    back = back[..., 0] + 1j * back[..., 1]
+    ref_i = oracle.ifft(xh.to(torch.complex128).cpu().numpy())
+    assert rel(back, ref_i) < 2e-3
+    lib.cfft_plan_destroy(h)
