@@ -22,6 +22,7 @@ const CFFT_FORWARD, CFFT_INVERSE, CFFT_BACKWARD = Cint(0), Cint(1), Cint(2)
 
 dtype_code(::Type{Float64}) = Cint(0)
 dtype_code(::Type{Float32}) = Cint(1)
+dtype_code(::Type{Float16}) = Cint(2)     # ComplexF16 data, FP32 arithmetic
 
 function check(rc::Cint)
     rc == 0 && return nothing
@@ -34,7 +35,7 @@ mutable struct Spell{T<:AbstractFloat}
     datatype::Type{T}
     flag::FLAG
     handle::Ptr{Cvoid}
-    function Spell(n::Int, ::Type{T}, flag::FLAG) where {T<:Union{Float32,Float64}}
+    function Spell(n::Int, ::Type{T}, flag::FLAG) where {T<:Union{Float16,Float32,Float64}}
         h = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:cfft_plan_create, LIB), Cint,
                     (Ref{Ptr{Cvoid}}, Int64, Int64, Cint, Cint),
@@ -59,24 +60,69 @@ function run!(y::Vector{Complex{T}}, p::Spell{T}, x::Vector{Complex{T}}, dir::Ci
     return y
 end
 
-fft(x::Vector{Complex{T}}) where {T<:Union{Float32,Float64}} =
-    run!(similar(x), getplan(length(x), T, NO_FLAG), x, CFFT_FORWARD)
-ifft(x::Vector{Complex{T}}) where {T<:Union{Float32,Float64}} =
-    run!(similar(x), getplan(length(x), T, NO_FLAG), x, CFFT_INVERSE)
-bfft(x::Vector{Complex{T}}) where {T<:Union{Float32,Float64}} =
-    run!(similar(x), getplan(length(x), T, NO_FLAG), x, CFFT_BACKWARD)
-fft!(x::Vector{Complex{T}}) where {T<:Union{Float32,Float64}} =
-    run!(x, getplan(length(x), T, NO_FLAG), x, CFFT_FORWARD)
+const Fl = Union{Float16,Float32,Float64}
+fft(x::Vector{Complex{T}}) where {T<:Fl} = run!(similar(x), getplan(length(x), T, NO_FLAG), x, CFFT_FORWARD)
+ifft(x::Vector{Complex{T}}) where {T<:Fl} = run!(similar(x), getplan(length(x), T, NO_FLAG), x, CFFT_INVERSE)
+bfft(x::Vector{Complex{T}}) where {T<:Fl} = run!(similar(x), getplan(length(x), T, NO_FLAG), x, CFFT_BACKWARD)
+fft!(x::Vector{Complex{T}}) where {T<:Fl} = run!(x, getplan(length(x), T, NO_FLAG), x, CFFT_FORWARD)
 
 plan_fft(x::Vector{Complex{T}}, flags::FLAG=NO_FLAG) where {T} = getplan(length(x), T, flags)
 mul!(y::Vector{Complex{T}}, p::Spell{T}, x::Vector{Complex{T}}) where {T} = run!(y, p, x, CFFT_FORWARD)
 *(p::Spell{T}, x::Vector{Complex{T}}) where {T} = run!(similar(x), p, x, CFFT_FORWARD)
+
+# real input: rfft / irfft / brfft (AbstractFFTs semantics; plan_rfft and
+# plan_brfft are stubs in the reference, src/CatabraFFT.jl:199-209)
+mutable struct RSpell{T<:AbstractFloat}
+    n::Int
+    handle::Ptr{Cvoid}
+    function RSpell(n::Int, ::Type{T}, flag::FLAG) where {T<:Union{Float32,Float64}}
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:cfft_rfft_plan_create, LIB), Cint, (Ref{Ptr{Cvoid}}, Int64, Int64, Cint, Cint),
+                    h, n, 1, dtype_code(T), Cint(flag)))
+        p = new{T}(n, h[])
+        finalizer(p) do q
+            q.handle != C_NULL && ccall((:cfft_rfft_plan_destroy, LIB), Cint, (Ptr{Cvoid},), q.handle)
+            q.handle = C_NULL
+        end
+        return p
+    end
+end
+const RPLANS = Dict{Tuple{Int,DataType,FLAG},RSpell}()
+getrplan(n::Int, ::Type{T}, flag::FLAG) where {T} = get!(() -> RSpell(n, T, flag), RPLANS, (n, T, flag))
+
+function rfft(x::Vector{T}) where {T<:Union{Float32,Float64}}
+    p = getrplan(length(x), T, NO_FLAG)
+    y = Vector{Complex{T}}(undef, length(x) ÷ 2 + 1)
+    check(ccall((:cfft_rfft_execute_host, LIB), Cint, (Ptr{Cvoid}, Ptr{T}, Ptr{Complex{T}}, Cint),
+                p.handle, x, y, CFFT_FORWARD))
+    return y
+end
+function _c2r(X::Vector{Complex{T}}, d::Int, dir::Cint) where {T<:Union{Float32,Float64}}
+    length(X) == d ÷ 2 + 1 || throw(DimensionMismatch("expected $(d ÷ 2 + 1) values for d=$d"))
+    p = getrplan(d, T, NO_FLAG)
+    y = Vector{T}(undef, d)
+    check(ccall((:cfft_rfft_execute_host, LIB), Cint, (Ptr{Cvoid}, Ptr{Complex{T}}, Ptr{T}, Cint),
+                p.handle, X, y, dir))
+    return y
+end
+irfft(X::Vector{Complex{T}}, d::Integer) where {T} = _c2r(X, Int(d), CFFT_INVERSE)
+brfft(X::Vector{Complex{T}}, d::Integer) where {T} = _c2r(X, Int(d), CFFT_BACKWARD)
+
+# wisdom: MEASURE / ENCHANT choices across sessions (the serialisable Spell
+# the reference sketched in src/spells.jl:180-375)
+export_wisdom(path::AbstractString) = check(ccall((:cfft_wisdom_export, LIB), Cint, (Cstring,), path))
+import_wisdom(path::AbstractString) = check(ccall((:cfft_wisdom_import, LIB), Cint, (Cstring,), path))
+forget_wisdom() = check(ccall((:cfft_wisdom_forget, LIB), Cint, ()))
 
 function empty_cache()
     for p in values(PLANS)
         finalize(p)
     end
     empty!(PLANS)
+    for p in values(RPLANS)
+        finalize(p)
+    end
+    empty!(RPLANS)
     check(ccall((:cfft_empty_cache, LIB), Cint, ()))
 end
 
