@@ -706,9 +706,10 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
 #pragma unroll 4
     for (int idx = tid; idx < R1 * N2; idx += T) {
         const int r = K::dN2(p, idx), k2 = idx - r * N2;
-        const int kk = (c * R1 + r) + N1 * k2;
+        // spectrum stored row-major for the cluster kernels: entry (k1, k2)
+        // at k1 N2 + k2, so this CTA's rows are contiguous
         V* e = bufC + r * PC + k2;
-        *e = conjv(fromd<V>(cmul(tod(*e), __ldg(p.spec + kk))));
+        *e = conjv(fromd<V>(cmul(tod(*e), __ldg(p.spec + (c * R1) * N2 + idx))));
     }
     __syncthreads();
     // ---- second FFT_M in transposed order: rows, twiddle + exchange, columns

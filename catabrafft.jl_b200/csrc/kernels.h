@@ -31,6 +31,7 @@ cudaError_t cfft_gen_bluestein_b(double2* b, const double2* ch, long long n, lon
 cudaError_t cfft_gen_rader_b(double2* b, const int* iperm, long long n, long long M, int exact,
                              double2 winv, cudaStream_t st);
 cudaError_t cfft_scale(double2* v, long long M, double s, cudaStream_t st);
+cudaError_t cfft_spec_rowmajor(double2* dst, const double2* src, long long N1, long long N2, cudaStream_t st);
 // real-input transforms (real.cu)
 cudaError_t cfft_r2c_post(void* out, long long N, long long n, long long batch, long long dist, int dtype,
                           cudaStream_t st);

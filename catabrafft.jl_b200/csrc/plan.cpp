@@ -680,7 +680,7 @@ static int conv_spectrum(cfft_plan_s* P, const std::string& key, int64_t M, G ge
     return rc;
 }
 
-static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp) {
+static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp, std::string* spec_key) {
     const int64_t n = P->n, M = sh.M;
     const std::string tag = std::to_string(n) + "/" + std::to_string(M);
     if (sh.conv == CONV_RADER) {
@@ -712,7 +712,8 @@ static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp) {
             winv = julia_inv(make_double2((double)cosl(x), (double)sinl(x)));
         }
         const int* iperm = kp.iperm;
-        return conv_spectrum(P, "sr/" + tag + "/" + std::to_string(exact), M, [&](double2* v) {
+        *spec_key = "sr/" + tag + "/" + std::to_string(exact);
+        return conv_spectrum(P, *spec_key, M, [&](double2* v) {
             return cfft_gen_rader_b(v, iperm, n, M, exact, winv, 0);
         }, &kp.spec);
     }
@@ -725,7 +726,8 @@ static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp) {
     if (rc) return rc;
     kp.chirp = (const double2*)dch;
     const double2* ch = kp.chirp;
-    return conv_spectrum(P, "sb/" + tag, M, [&](double2* v) {
+    *spec_key = "sb/" + tag;
+    return conv_spectrum(P, *spec_key, M, [&](double2* v) {
         return cfft_gen_bluestein_b(v, ch, n, M, 0);
     }, &kp.spec);
 }
@@ -742,8 +744,22 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     kp.M = (int)sh.M;
     int rc;
     if (sh.conv != CONV_NONE) {
-        rc = make_conv_tables(P, sh, kp);
+        std::string spec_key;
+        rc = make_conv_tables(P, sh, kp, &spec_key);
         if (rc) return rc;
+        if (sh.mode == MODE_FOUR) {
+            // the cluster kernels read the spectrum in row-major (k1, k2) order
+            const double2* nat = kp.spec;
+            const void* d = nullptr;
+            const int64_t N1 = sh.N1, N2 = sh.N2;
+            rc = cached_dev_table(P, spec_key + "/rm" + std::to_string(N1), (size_t)sh.M * sizeof(double2),
+                                  [&](void* dp) -> int {
+                                      CUDA_TRY(cfft_spec_rowmajor((double2*)dp, nat, N1, N2, 0));
+                                      return CFFT_OK;
+                                  }, &d);
+            if (rc) return rc;
+            kp.spec = (const double2*)d;
+        }
     }
     if (sh.mode == MODE_ROWS) {
         kp.mode = MODE_ROWS;

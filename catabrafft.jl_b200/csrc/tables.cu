@@ -108,3 +108,18 @@ cudaError_t cfft_scale(double2* v, long long M, double s, cudaStream_t st) {
     k_scale<<<grid_for(M), 256, 0, st>>>(v, M, s);
     return cudaGetLastError();
 }
+
+// spectrum in the cluster kernels' row-major (k1, k2) order: dst[k1 N2 + k2]
+// = src[k1 + N1 k2], so each CTA reads its rows contiguously
+__global__ void k_spec_rowmajor(double2* dst, const double2* src, long long N1, long long N2) {
+    const long long M = N1 * N2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long k1 = i / N2, k2 = i - k1 * N2;
+        dst[i] = src[k1 + N1 * k2];
+    }
+}
+cudaError_t cfft_spec_rowmajor(double2* dst, const double2* src, long long N1, long long N2, cudaStream_t st) {
+    k_spec_rowmajor<<<grid_for(N1 * N2), 256, 0, st>>>(dst, src, N1, N2);
+    return cudaGetLastError();
+}
