@@ -666,18 +666,22 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             x0 = r0[0];
         }
         const int L = nx - 1;
+        // p.perm is in this kernel's order: entry c*N1*W + idx holds
+        // (owner << 24 | offset) of x[g^jj] in the owners' x chunks, or -1 for
+        // the zero padding (jj >= L)
+        const int* pc = p.perm + c * (N1 * W);
 #pragma unroll 4
         for (int idx = tid; idx < N1 * W; idx += T) {
             const int i1 = K::dW(p, idx), j = idx - i1 * W;
-            const int jj = i1 * N2 + c * W + j;
+            const int code = __ldg(pc + idx);
             V v = zero<V>();
-            if (jj < L) {
-                const int src = __ldg(p.perm + jj), owner = fdiv(src, p.mX);
-                const V* rx = (C > 1) ? cl.map_shared_rank(xs, owner) : xs;
-                v = rx[src - owner * XC];
+            if (code >= 0) {
+                const V* rx = (C > 1) ? cl.map_shared_rank(xs, code >> 24) : xs;
+                v = rx[code & 0xffffff];
             }
             buf[i1 * PA + j] = v;
         }
+        (void)L;
     }
     __syncthreads();
     // the idle buffer is free: nobody reads it any more (its last remote
@@ -738,17 +742,20 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     // xs was last read in the prologue (the gather and x0); the exchanges'
     // cluster barriers since then order those reads before these writes
     if (C == 1) __syncthreads();
+    // p.iperm in this kernel's order, coded like p.perm: the owner and
+    // offset of y[g^-jj] in the x chunks
+    const int* ic = p.iperm + c * (N1 * W);
 #pragma unroll 4
     for (int idx = tid; idx < N1 * W; idx += T) {
         const int j1 = K::dW(p, idx), j = idx - j1 * W;
-        const int jj = j1 * N2 + c * W + j;
-        if (jj < L) {
+        const int code = __ldg(ic + idx);
+        if (code >= 0) {
             const V cv = conjv(buf[j1 * PA + j]);
-            const int dst = __ldg(p.iperm + jj), owner = fdiv(dst, p.mX);
-            V* rx = (C > 1) ? cl.map_shared_rank(xs, owner) : xs;
-            rx[dst - owner * XC] = mk<V>(x0.x + cv.x, x0.y + cv.y);
+            V* rx = (C > 1) ? cl.map_shared_rank(xs, code >> 24) : xs;
+            rx[code & 0xffffff] = mk<V>(x0.x + cv.x, x0.y + cv.y);
         }
     }
+    (void)L;
     if (C > 1) cl.sync(); else __syncthreads();
     if (c == 0 && tid == 0) {
         double2 d = tod(x0);

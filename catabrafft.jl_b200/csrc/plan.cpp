@@ -747,6 +747,41 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         std::string spec_key;
         rc = make_conv_tables(P, sh, kp, &spec_key);
         if (rc) return rc;
+        if (sh.mode == MODE_FOUR && sh.conv == CONV_RADER) {
+            // the cluster kernels read the permutations in their own order:
+            // entry c*N1*W + i1*W + j for position jj = i1*N2 + c*W + j holds
+            // (owner << 24 | offset) of g^(+-jj) within the C x chunks of
+            // ceil(n/C) elements, or -1 for the zero padding jj >= n - 1
+            const int64_t n = P->n, L = n - 1, N1 = sh.N1, N2 = sh.N2, C = sh.C, W = N2 / C;
+            const int64_t XC = (n + C - 1) / C;
+            const void* d = nullptr;
+            rc = cached_table(P, "pmc/" + std::to_string(n) + "/" + std::to_string(N1) + "/" + std::to_string(N2) +
+                                     "/" + std::to_string(C),
+                              [&](std::vector<unsigned char>& img) {
+                const int64_t g = primitive_root(n), ginv = powmod(g, n - 2, n);
+                std::vector<int> fw(L), bw(L);
+                int64_t a = 1, b = 1;
+                for (int64_t i = 0; i < L; i++) {
+                    fw[i] = (int)a;
+                    bw[i] = (int)b;
+                    a = (int64_t)(((__int128)a * g) % n);
+                    b = (int64_t)(((__int128)b * ginv) % n);
+                }
+                std::vector<int> v(2 * (size_t)N1 * N2);
+                for (int64_t c = 0; c < C; c++)
+                    for (int64_t i1 = 0; i1 < N1; i1++)
+                        for (int64_t j = 0; j < W; j++) {
+                            const int64_t jj = i1 * N2 + c * W + j, at = c * N1 * W + i1 * W + j;
+                            auto code = [&](int64_t s) { return (int)(((s / XC) << 24) | (s % XC)); };
+                            v[at] = jj < L ? code(fw[jj]) : -1;
+                            v[N1 * N2 + at] = jj < L ? code(bw[jj]) : -1;
+                        }
+                put(img, v);
+            }, &d);
+            if (rc) return rc;
+            kp.perm = (const int*)d;
+            kp.iperm = (const int*)d + N1 * N2;
+        }
         if (sh.mode == MODE_FOUR) {
             // the cluster kernels read the spectrum in row-major (k1, k2) order
             const double2* nat = kp.spec;
