@@ -37,7 +37,7 @@ PLANNER_DEFAULT = NO_FLAG
 __all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_cache", "Batch", "Server",
            "export_wisdom", "import_wisdom", "forget_wisdom", "wisdom_entries",
            "rfft", "irfft", "brfft", "plan_rfft", "plan_brfft", "RSpell", "plan_bfft", "plan_ifft",
-           "plan_inv",
+           "plan_inv", "fftn", "ifftn", "fft2", "ifft2",
            "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
            "describe_strategy", "version"]
 
@@ -158,19 +158,104 @@ def _run(x, direction: int, flags: int = NO_FLAG, out=None):
     return y
 
 
-def fft(x):
-    """Forward DFT along the last axis (CatabraFFT.fft)."""
-    return _run(x, FORWARD)
+def _run_axis(x, direction: int, axis: int):
+    """Transform along one axis of an N-D array (the reference's `region`,
+    ignored there at CatabraFFT.jl:169).  CUDA tensors use strided plans
+    (cfft_plan_create_many): the axis has stride `inner`, the transforms of
+    one outer index are `inner` apart by 1; host arrays are transposed on the
+    host around the contiguous path."""
+    nd = x.dim() if _is_torch(x) else np.ndim(x)
+    if not -nd <= axis < nd:
+        raise ValueError(f"axis {axis} out of range for a {nd}-D array")
+    axis = axis % nd
+    if axis == nd - 1:
+        if nd <= 2:
+            return _run(x, direction)
+        if _is_torch(x):
+            return _run(x.reshape(-1, x.shape[-1]), direction).reshape(x.shape)
+        a = np.asarray(x)
+        return _run(a.reshape(-1, a.shape[-1]), direction).reshape(a.shape)
+    if _is_torch(x) and x.is_cuda:
+        import torch
+        xc = x.contiguous()
+        shape = list(xc.shape)
+        n = shape[axis]
+        outer = int(np.prod(shape[:axis])) if axis else 1
+        inner = int(np.prod(shape[axis + 1:]))
+        y = torch.empty_like(xc)
+        dt = _dtype_code(xc.dtype)
+        e = 16 if dt == C128 else 8
+        key = ("many", xc.device.index, n, inner, dt)
+        with _cache_lock:
+            h = _plans.get(key)
+            if h is None:
+                hp = ctypes.c_void_p()
+                check(_lib.LIB.cfft_plan_create_many(ctypes.byref(hp), n, inner, dt, NO_FLAG, inner, 1, inner, 1))
+                h = _ManyPlan(hp)
+                _plans[key] = h
+        stream = ctypes.c_void_p(torch.cuda.current_stream(xc.device).cuda_stream)
+        with torch.cuda.device(xc.device):
+            for o in range(outer):
+                off = o * n * inner * e
+                check(_lib.LIB.cfft_execute(h.handle, ctypes.c_void_p(xc.data_ptr() + off),
+                                            ctypes.c_void_p(y.data_ptr() + off), direction, stream))
+        return y
+    if _is_torch(x):
+        import torch
+        return torch.from_numpy(_run_axis(x.detach().numpy(), direction, axis))
+    a = np.moveaxis(np.asarray(x), axis, -1)
+    return np.moveaxis(_run_axis(np.ascontiguousarray(a), direction, -1), -1, axis)
 
 
-def ifft(x):
+class _ManyPlan:
+    def __init__(self, handle):
+        self.handle = handle
+
+    def destroy(self):
+        if self.handle:
+            _lib.LIB.cfft_plan_destroy(self.handle)
+            self.handle = None
+
+
+def fft(x, axis: int = -1):
+    """Forward DFT along `axis` (default the last; CatabraFFT.fft)."""
+    return _run(x, FORWARD) if axis == -1 and np.ndim(x) <= 2 and not (_is_torch(x) and x.dim() > 2) \
+        else _run_axis(x, FORWARD, axis)
+
+
+def ifft(x, axis: int = -1):
     """Inverse DFT scaled by 1/n (CatabraFFT.ifft: conj, fft, conj, /n)."""
-    return _run(x, INVERSE)
+    return _run(x, INVERSE) if axis == -1 and np.ndim(x) <= 2 and not (_is_torch(x) and x.dim() > 2) \
+        else _run_axis(x, INVERSE, axis)
 
 
-def bfft(x):
+def bfft(x, axis: int = -1):
     """Unscaled inverse DFT (CatabraFFT.bfft)."""
-    return _run(x, BACKWARD)
+    return _run(x, BACKWARD) if axis == -1 and np.ndim(x) <= 2 and not (_is_torch(x) and x.dim() > 2) \
+        else _run_axis(x, BACKWARD, axis)
+
+
+def fftn(x, axes=None):
+    """Multi-dimensional DFT: one pass per axis (default all axes)."""
+    nd = x.dim() if _is_torch(x) else np.ndim(x)
+    for a in (range(nd) if axes is None else axes):
+        x = _run_axis(x, FORWARD, a)
+    return x
+
+
+def ifftn(x, axes=None):
+    nd = x.dim() if _is_torch(x) else np.ndim(x)
+    for a in (range(nd) if axes is None else axes):
+        x = _run_axis(x, INVERSE, a)
+    return x
+
+
+def fft2(x):
+    return fftn(x, (-2, -1))
+
+
+def ifft2(x):
+    return ifftn(x, (-2, -1))
 
 
 def fft_(x):

@@ -46,6 +46,7 @@ SIGNATURES = {
     "cfft_serve_drain": (_ci, [_vp]),
     "cfft_serve_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "cfft_serve_destroy": (_ci, [_vp]),
+    "cfft_plan_create_many": (_ci, [ctypes.POINTER(_vp), _i64, _i64, _ci, _ci, _i64, _i64, _i64, _i64]),
     "cfft_rfft_plan_create": (_ci, [ctypes.POINTER(_vp), _i64, _i64, _ci, _ci]),
     "cfft_rfft_execute": (_ci, [_vp, _vp, _vp, _vp]),
     "cfft_rfft_execute_inverse": (_ci, [_vp, _vp, _vp, _ci, _vp]),

@@ -45,5 +45,10 @@ cudaError_t cfft_c2r_real(const void* s, void* x, long long n, long long batch, 
 // ComplexF16 <-> ComplexF32 element conversion (real.cu)
 cudaError_t cfft_half_to_float(const void* in, void* out, long long count, cudaStream_t st);
 cudaError_t cfft_float_to_half(const void* in, void* out, long long count, cudaStream_t st);
+// strided layouts <-> contiguous working buffer (real.cu)
+cudaError_t cfft_gather(const void* in, void* w, long long n, long long batch, long long stride, long long dist,
+                        int dtype, cudaStream_t st);
+cudaError_t cfft_scatter(const void* w, void* out, long long n, long long batch, long long stride, long long dist,
+                         int dtype, cudaStream_t st);
 // set the thread-local text returned by cfft_last_error() (fixed buffer)
 void cfft_set_last_error(const char* msg);

@@ -275,6 +275,11 @@ struct cfft_plan_s {
     void* host_buf[3] = {nullptr, nullptr, nullptr};
     cudaStream_t host_st[3] = {nullptr, nullptr, nullptr};   // in, compute, out
     cudaEvent_t ev_in[3], ev_comp[3], ev_out[3];
+    // strided plans (cfft_plan_create_many): element i of transform b at
+    // b * dist + i * stride; gathered into / scattered from strided_work
+    bool strided = false;
+    int64_t istride = 1, idist = 0, ostride = 1, odist = 0;
+    void* strided_work = nullptr;
     // ComplexF16 plans: ComplexF16 in/out around the ComplexF32 path
     bool io_half = false;
     void* half_work = nullptr;   // batch * n ComplexF32
@@ -1899,9 +1904,51 @@ static int execute_half(cfft_plan_s* P, const void* d_in, void* d_out, int direc
     return CFFT_OK;
 }
 
+static int execute_strided(cfft_plan_s* P, const void* d_in, void* d_out, int direction, cudaStream_t st) {
+    if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
+    const size_t e = elem_bytes(P->dtype);
+    if (((uintptr_t)d_in % e) != 0 || ((uintptr_t)d_out % e) != 0)
+        return fail(CFFT_ERR_INVALID, "buffers must be aligned to the element size");
+    CUDA_TRY(cfft_gather(d_in, P->strided_work, P->n, P->batch, P->istride, P->idist, P->dtype, st));
+    int rc = plan_execute(P, P->strided_work, P->strided_work, direction, st);
+    if (rc) return rc;
+    CUDA_TRY(cfft_scatter(P->strided_work, d_out, P->n, P->batch, P->ostride, P->odist, P->dtype, st));
+    return CFFT_OK;
+}
+
+int cfft_plan_create_many(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags, int64_t istride,
+                          int64_t idist, int64_t ostride, int64_t odist) {
+    g_err[0] = 0;
+    if (!plan) return fail(CFFT_ERR_INVALID, "plan pointer is null");
+    if (istride < 1 || ostride < 1 || idist < 0 || odist < 0)
+        return fail(CFFT_ERR_INVALID, "strides must be >= 1 and distances >= 0");
+    if (dtype != CFFT_C128 && dtype != CFFT_C64)
+        return fail(CFFT_ERR_INVALID, "strided plans take CFFT_C128 or CFFT_C64");
+    int rc = plan_create_impl(plan, n, batch, dtype, flags);
+    if (rc) return rc;
+    cfft_plan_s* P = *plan;
+    if (istride == 1 && ostride == 1 && (idist == n || batch == 1) && (odist == n || batch == 1)) return CFFT_OK;
+    P->strided = true;
+    P->istride = istride;
+    P->idist = idist;
+    P->ostride = ostride;
+    P->odist = odist;
+    if (cudaMalloc(&P->strided_work, (size_t)n * batch * elem_bytes(dtype)) != cudaSuccess) {
+        cudaGetLastError();
+        plan_free(P);
+        delete P;
+        *plan = nullptr;
+        return fail(CFFT_ERR_NOMEM, "strided working buffer allocation failed");
+    }
+    P->allocs.push_back(P->strided_work);
+    P->desc = "strided+" + P->desc;
+    return CFFT_OK;
+}
+
 int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, void* stream) {
     if (!plan || !d_in || !d_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (plan->io_half) return execute_half(plan, d_in, d_out, direction, (cudaStream_t)stream);
+    if (plan->strided) return execute_strided(plan, d_in, d_out, direction, (cudaStream_t)stream);
     return plan_execute(plan, d_in, d_out, direction, (cudaStream_t)stream);
 }
 
@@ -1909,6 +1956,7 @@ int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int directi
     if (!plan || !h_in || !h_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
     cfft_plan_s* P = plan;
+    if (P->strided) return fail(CFFT_ERR_UNSUPPORTED, "strided plans take device buffers (cfft_execute)");
     std::lock_guard<std::mutex> lk(P->host_mu);
     if (P->io_half) {
         const size_t bytes = (size_t)P->n * P->batch * 4;

@@ -170,3 +170,34 @@ cudaError_t cfft_float_to_half(const void* in, void* out, long long count, cudaS
     k_f2h<<<grid_for(count), 256, 0, st>>>((const float2*)in, (__half2*)out, count);
     return cudaGetLastError();
 }
+
+// strided layouts: element i of transform b at base[b * dist + i * stride]
+// gathered into / scattered out of a contiguous [batch][n] working buffer
+template <typename V>
+__global__ void k_gather(const V* in, V* w, long long n, long long batch, long long stride, long long dist) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * batch;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long b = i / n, k = i - b * n;
+        w[i] = in[b * dist + k * stride];
+    }
+}
+template <typename V>
+__global__ void k_scatter(const V* w, V* out, long long n, long long batch, long long stride, long long dist) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * batch;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long b = i / n, k = i - b * n;
+        out[b * dist + k * stride] = w[i];
+    }
+}
+cudaError_t cfft_gather(const void* in, void* w, long long n, long long batch, long long stride, long long dist,
+                        int dtype, cudaStream_t st) {
+    if (dtype == CFFT_DT_C128) k_gather<double2><<<grid_for(n * batch), 256, 0, st>>>((const double2*)in, (double2*)w, n, batch, stride, dist);
+    else k_gather<float2><<<grid_for(n * batch), 256, 0, st>>>((const float2*)in, (float2*)w, n, batch, stride, dist);
+    return cudaGetLastError();
+}
+cudaError_t cfft_scatter(const void* w, void* out, long long n, long long batch, long long stride, long long dist,
+                         int dtype, cudaStream_t st) {
+    if (dtype == CFFT_DT_C128) k_scatter<double2><<<grid_for(n * batch), 256, 0, st>>>((const double2*)w, (double2*)out, n, batch, stride, dist);
+    else k_scatter<float2><<<grid_for(n * batch), 256, 0, st>>>((const float2*)w, (float2*)out, n, batch, stride, dist);
+    return cudaGetLastError();
+}

@@ -71,6 +71,16 @@ int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, v
  * out and synchronises.  Host buffers may be pageable or pinned. */
 int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int direction);
 
+/* Strided layouts -- the reference's `region` argument, which it ignores
+ * (src/CatabraFFT.jl:169): element i of transform b is read at
+ * d_in[b * idist + i * istride] and written at d_out[b * odist + i * ostride]
+ * (elements, not bytes).  Transforming the second axis of a column-major
+ * n1 x n2 Julia matrix is n = n2, batch = n1, stride = n1, dist = 1.  The
+ * data is gathered into a contiguous working buffer, transformed and
+ * scattered back; cfft_execute only (device buffers). */
+int cfft_plan_create_many(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags, int64_t istride,
+                          int64_t idist, int64_t ostride, int64_t odist);
+
 /* Releases a plan and its device tables. */
 int cfft_plan_destroy(cfft_plan plan);
 

@@ -68,7 +68,7 @@ def test_python_api_argument_errors():
     with pytest.raises(TypeError):
         m.fft(np.zeros(8, dtype=np.float64))
     with pytest.raises(ValueError):
-        m.fft(np.zeros((2, 2, 2), dtype=np.complex128))
+        m.fft(np.zeros((2, 2), dtype=np.complex128), axis=2)
     with pytest.raises(ValueError):
         m.plan_fft(np.zeros(8, dtype=np.complex128), 3)
 

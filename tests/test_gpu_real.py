@@ -120,3 +120,42 @@ def test_complex_f16(cb):
     ref_i = oracle.ifft(xh.to(torch.complex128).cpu().numpy())
     assert rel(back, ref_i) < 2e-3
     lib.cfft_plan_destroy(h)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_axes_and_multidim(cb, dtype):
+    """Strided plans (the reference's ignored `region`): transforms along any
+    axis of device tensors, fft2/fftn; host arrays through host transposes."""
+    import torch
+    rng = np.random.default_rng(21)
+    x = (rng.standard_normal((6, 30240 // 6 // 7, 7 * 6)) + 1j * rng.standard_normal((6, 720, 42))).astype(dtype)
+    tol = 1e-12 if dtype == np.complex128 else 1e-5
+    xd = torch.from_numpy(x).cuda()
+    for axis in (0, 1, 2, -1):
+        ref = np.fft.fft(x.astype(np.complex128), axis=axis)
+        assert rel(cb.fft(xd, axis=axis).cpu().numpy(), ref) < tol, axis
+        assert rel(cb.fft(x, axis=axis), ref) < tol, axis
+    ref2 = np.fft.fft2(x.astype(np.complex128))
+    assert rel(cb.fft2(xd).cpu().numpy(), ref2) < 2 * tol
+    refn = np.fft.fftn(x.astype(np.complex128))
+    assert rel(cb.fftn(xd).cpu().numpy(), refn) < 3 * tol
+    assert rel(cb.ifftn(cb.fftn(xd)).cpu().numpy(), x) < 6 * tol
+
+
+def test_plan_many_strided_abi(cb):
+    """cfft_plan_create_many through the C ABI: the second axis of a
+    column-major n1 x n2 matrix (stride n1, distance 1)."""
+    import ctypes
+    import torch
+    n1, n2 = 96, 1000
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((n2, n1)) + 1j * rng.standard_normal((n2, n1))   # row-major view of column-major n1 x n2
+    d = torch.from_numpy(A).cuda()
+    y = torch.empty_like(d)
+    lib = cb._lib.LIB
+    h = ctypes.c_void_p()
+    cb.check(lib.cfft_plan_create_many(ctypes.byref(h), n2, n1, cb.C128, 0, n1, 1, n1, 1))
+    cb.check(lib.cfft_execute(h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(y.data_ptr()), 0,
+                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    assert rel(y.cpu().numpy(), np.fft.fft(A, axis=0)) < 1e-12
+    lib.cfft_plan_destroy(h)
