@@ -665,7 +665,6 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             const V* r0 = (C > 1) ? cl.map_shared_rank(xs, 0) : xs;
             x0 = r0[0];
         }
-        const int L = nx - 1;
         // p.perm is in this kernel's order: entry c*N1*W + idx holds
         // (owner << 24 | offset) of x[g^jj] in the owners' x chunks, or -1 for
         // the zero padding (jj >= L)
@@ -681,7 +680,6 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             }
             buf[i1 * PA + j] = v;
         }
-        (void)L;
     }
     __syncthreads();
     // the idle buffer is free: nobody reads it any more (its last remote
@@ -738,7 +736,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     }
 
     // Rader epilogue: y[g^-j] = x0 + c[j]; y[0] = x0 + sum(x[1:])
-    const int XC = p.XP, L = nx - 1;
+    const int XC = p.XP;
     // xs was last read in the prologue (the gather and x0); the exchanges'
     // cluster barriers since then order those reads before these writes
     if (C == 1) __syncthreads();
@@ -755,7 +753,6 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             rx[code & 0xffffff] = mk<V>(x0.x + cv.x, x0.y + cv.y);
         }
     }
-    (void)L;
     if (C > 1) cl.sync(); else __syncthreads();
     if (c == 0 && tid == 0) {
         double2 d = tod(x0);
