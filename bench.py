@@ -44,6 +44,20 @@ def flops_per_step():
     return sum(2 * b * 5 * n * np.log2(n) for n, b in SIZES)
 
 
+def max_over_ranks(torch, value, device):
+    """The largest of every rank's value (device-timed milliseconds): the
+    replicas' job time is the slowest rank's."""
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.item()
+
+
+def job_gbs(world, bytes_per_rank_step, ms_step):
+    """Whole-job throughput of `world` replicas: every rank moves the same
+    bytes per step, the step takes the slowest rank's time."""
+    return world * bytes_per_rank_step / (ms_step * 1e-3) / 1e9
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -204,9 +218,7 @@ def measure_e2e(torch, cb, lib, plans, bufs, args, world, dev):
             cb.check(lib.cfft_execute_host(h, vp(hout.data_ptr()), vp(hout.data_ptr()), 1))
     e2e_s = (time.perf_counter() - te) / steps
     if world > 1:
-        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = tt.item()
+        e2e_s = max_over_ranks(torch, e2e_s, dev)
     # per step: 2 calls per batch, each copies the batch in and out
     io_bytes = sum(2 * n * b * ELEM for n, b in SIZES)
     return {"value": round(world * algorithmic_bytes_per_step() / e2e_s / 1e9, 4), "unit": "GB/s",
@@ -596,11 +608,9 @@ def main():
         torch.distributed.barrier()
     ms = t0.elapsed_time(t1)
     if world > 1:
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = tt.item()
+        ms = max_over_ranks(torch, ms, dev)
     ms_step = ms / args.steps
-    value = world * algorithmic_bytes_per_step() / (ms_step * 1e-3) / 1e9
+    value = job_gbs(world, algorithmic_bytes_per_step(), ms_step)
 
     # per-launch kernel time (each cfft_execute of these plans is one launch)
     per = []
