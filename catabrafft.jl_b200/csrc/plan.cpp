@@ -275,6 +275,8 @@ struct cfft_plan_s {
     void* host_buf[3] = {nullptr, nullptr, nullptr};
     cudaStream_t host_st[3] = {nullptr, nullptr, nullptr};   // in, compute, out
     cudaEvent_t ev_in[3], ev_comp[3], ev_out[3];
+    void* stage_in[3] = {nullptr, nullptr, nullptr};    // pinned staging for pageable callers
+    void* stage_out[3] = {nullptr, nullptr, nullptr};
     // strided plans (cfft_plan_create_many): element i of transform b at
     // b * dist + i * stride; gathered into / scattered from strided_work
     bool strided = false;
@@ -984,6 +986,9 @@ static void plan_free(cfft_plan_s* P) {
             cudaEventDestroy(P->ev_comp[i]);
             cudaEventDestroy(P->ev_out[i]);
             P->host_buf[i] = nullptr;
+            if (P->stage_in[i]) cudaFreeHost(P->stage_in[i]);
+            if (P->stage_out[i]) cudaFreeHost(P->stage_out[i]);
+            P->stage_in[i] = P->stage_out[i] = nullptr;
         }
         P->host_ready = false;
     }
@@ -1952,6 +1957,83 @@ int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, v
     return plan_execute(plan, d_in, d_out, direction, (cudaStream_t)stream);
 }
 
+// page-locked (or otherwise DMA-able) host memory?
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+// memcpy split over a few threads (pageable <-> pinned staging)
+static void par_memcpy(void* dst, const void* src, size_t bytes) {
+    const size_t kMin = (size_t)4 << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, bytes / kMin));
+    if (nt <= 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t step = (bytes + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        const size_t a = t * step, b = std::min(bytes, a + step);
+        if (a < b) th.emplace_back([=] { memcpy((char*)dst + a, (const char*)src + a, b - a); });
+    }
+    for (auto& x : th) x.join();
+}
+// Pageable host buffers (a Julia Vector, a numpy array): the chunks pass
+// through pinned staging buffers; the CPU copies chunk i in (and chunk i-3
+// out) while the GPU moves and transforms the chunks in between.
+static int execute_host_staged(cfft_plan_s* P, const void* h_in, void* h_out, int direction, size_t tbytes) {
+    cudaStream_t sin = P->host_st[0], scomp = P->host_st[1], sout = P->host_st[2];
+    const size_t cap = (size_t)P->host_chunk * tbytes;
+    for (int k = 0; k < 3; k++) {
+        if (!P->stage_in[k]) CUDA_TRY(cudaHostAlloc(&P->stage_in[k], cap, cudaHostAllocDefault));
+        if (!P->stage_out[k]) CUDA_TRY(cudaHostAlloc(&P->stage_out[k], cap, cudaHostAllocDefault));
+    }
+    const int64_t nch = (P->batch + P->host_chunk - 1) / P->host_chunk;
+    auto span = [&](int64_t i, size_t* off, size_t* bytes) {
+        const int64_t b0 = i * P->host_chunk, nb = std::min(P->host_chunk, P->batch - b0);
+        *off = (size_t)b0 * tbytes;
+        *bytes = (size_t)nb * tbytes;
+    };
+    auto drain = [&](int64_t i) -> int {          // chunk i's result to the caller
+        const int k = (int)(i % 3);
+        size_t off, bytes;
+        span(i, &off, &bytes);
+        CUDA_TRY(cudaEventSynchronize(P->ev_out[k]));
+        par_memcpy((char*)h_out + off, P->stage_out[k], bytes);
+        return CFFT_OK;
+    };
+    for (int64_t i = 0; i < nch; i++) {
+        const int k = (int)(i % 3);
+        size_t off, bytes;
+        span(i, &off, &bytes);
+        if (i >= 3) {
+            int rc = drain(i - 3);                 // frees stage_in/out[k] and host_buf[k]
+            if (rc) return rc;
+        }
+        par_memcpy(P->stage_in[k], (const char*)h_in + off, bytes);
+        CUDA_TRY(cudaMemcpyAsync(P->host_buf[k], P->stage_in[k], bytes, cudaMemcpyHostToDevice, sin));
+        CUDA_TRY(cudaEventRecord(P->ev_in[k], sin));
+        CUDA_TRY(cudaStreamWaitEvent(scomp, P->ev_in[k], 0));
+        int rc = plan_execute(P, P->host_buf[k], P->host_buf[k], direction, scomp, (int64_t)(bytes / tbytes));
+        if (rc) { cudaStreamSynchronize(scomp); return rc; }
+        CUDA_TRY(cudaEventRecord(P->ev_comp[k], scomp));
+        CUDA_TRY(cudaStreamWaitEvent(sout, P->ev_comp[k], 0));
+        CUDA_TRY(cudaMemcpyAsync(P->stage_out[k], P->host_buf[k], bytes, cudaMemcpyDeviceToHost, sout));
+        CUDA_TRY(cudaEventRecord(P->ev_out[k], sout));
+    }
+    for (int64_t i = std::max<int64_t>(0, nch - 3); i < nch; i++) {
+        int rc = drain(i);
+        if (rc) return rc;
+    }
+    CUDA_TRY(cudaStreamSynchronize(scomp));
+    return CFFT_OK;
+}
+
 int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int direction) {
     if (!plan || !h_in || !h_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
@@ -1990,6 +2072,7 @@ int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int directi
     // three-stage pipeline: H2D (stream 0) -> transform (stream 1) -> D2H
     // (stream 2) over a ring of three device chunk buffers
     cudaStream_t sin = P->host_st[0], scomp = P->host_st[1], sout = P->host_st[2];
+    if (!host_pinned(h_in) || !host_pinned(h_out)) return execute_host_staged(P, h_in, h_out, direction, tbytes);
     int64_t i = 0;
     for (int64_t b0 = 0; b0 < P->batch; b0 += P->host_chunk, i++) {
         const int64_t nb = std::min(P->host_chunk, P->batch - b0);

@@ -68,7 +68,9 @@ int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, v
 
 /* Replaces fft(x) / ifft(x) / bfft(x) (src/CatabraFFT.jl:65-115) for callers
  * holding host memory (the Julia ccall path): copies in, transforms, copies
- * out and synchronises.  Host buffers may be pageable or pinned. */
+ * out and synchronises.  Host buffers may be pinned (copied by DMA directly)
+ * or pageable (staged through the plan's pinned buffers by host threads,
+ * overlapped with the device work). */
 int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int direction);
 
 /* Strided layouts -- the reference's `region` argument, which it ignores
