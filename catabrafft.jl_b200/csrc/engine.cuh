@@ -855,7 +855,8 @@ __device__ __forceinline__ bool colpass_fix(const KParams& p, int tile, V* buf) 
 // column FFTs and the twiddled store; (c0 + j) * k1 < N2 * N1 = M, so the
 // exponent needs no reduction
 template <typename V, int EMAX>
-__device__ __forceinline__ void colpass_finish(const KParams& p, int tile, V* buf, const V* tw) {
+__device__ __forceinline__ void colpass_finish(const KParams& p, int tile, V* buf, const V* tw,
+                                               const TwoLevel& t4) {
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
     V* out = (V*)p.out + (long long)t * p.out_dist;
@@ -868,13 +869,13 @@ __device__ __forceinline__ void colpass_finish(const KParams& p, int tile, V* bu
         V* o = out + c0 + j;
 #pragma unroll 4
         for (int k1 = tid / Vw; k1 < N1; k1 += ks)
-            o[(long long)k1 * N2] = apply_tw(buf[k1 * PA + j], p.t4, c * (unsigned)k1);
+            o[(long long)k1 * N2] = apply_tw(buf[k1 * PA + j], t4, c * (unsigned)k1);
     } else {
 #pragma unroll 4
         for (int idx = tid; idx < total; idx += T) {
             const int k1 = fdiv(idx, p.mV), j = idx - k1 * Vw;
             const unsigned e = (unsigned)(c0 + j) * (unsigned)k1;
-            out[(long long)k1 * N2 + c0 + j] = apply_tw(buf[k1 * PA + j], p.t4, e);
+            out[(long long)k1 * N2 + c0 + j] = apply_tw(buf[k1 * PA + j], t4, e);
         }
     }
 }
@@ -920,15 +921,23 @@ __device__ __forceinline__ void colpass_body(const KParams& p, unsigned char* sm
     const int tile = block_id(p);
     if (tile >= p.batch * (p.N2 / p.V)) return;
     const int lt = cfft_pass_tw_elems(p.pa.twlen, (int)sizeof(V));
+    const int nt = cfft_pass_t4_elems(p.t4.bits, p.t4.N), nlo = 1 << p.t4.bits;
     V* tws = (V*)smem;
-    V* buf = tws + lt;
+    double2* t4s = after16(tws + lt);
+    V* buf = (V*)(t4s + nt);
     colpass_issue<V>(p, tile, buf);
     cp_async_commit();
     for (int i = tid; i < lt; i += T) tws[i] = ((const V*)p.pa.tw)[i];
+    for (int i = tid; i < nt; i += T) t4s[i] = (i < nlo) ? p.t4.lo[i] : p.t4.hi[i - nlo];
+    TwoLevel t4 = p.t4;
+    if (nt) {
+        t4.lo = t4s;
+        t4.hi = t4s + nlo;
+    }
     cp_async_wait_all();
     __syncthreads();
     if (colpass_fix<V>(p, tile, buf)) __syncthreads();
-    colpass_finish<V, EMAX>(p, tile, buf, lt ? (const V*)tws : (const V*)p.pa.tw);
+    colpass_finish<V, EMAX>(p, tile, buf, lt ? (const V*)tws : (const V*)p.pa.tw, t4);
 }
 template <typename V, int EMAX>
 __device__ __forceinline__ void rowpass_body(const KParams& p, unsigned char* smem) {

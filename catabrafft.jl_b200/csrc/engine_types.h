@@ -77,6 +77,17 @@ inline __host__ __device__ bool cfft_pass_tw_staged(int twlen, int elem_bytes) {
 inline __host__ __device__ int cfft_pass_tw_elems(int twlen, int elem_bytes) {
     return cfft_pass_tw_staged(twlen, elem_bytes) ? twlen : 0;
 }
+// COLPASS also stages the two-level four-step table (FP64 lo then hi, after
+// the sub-transform table, 16-byte aligned) when it is at most 12 KB
+inline __host__ __device__ int cfft_pass_t4_elems(int bits, int N) {
+    const int nlo = 1 << bits, nhi = (N + nlo - 1) / nlo + 1;
+    return (nlo + nhi) * 16 <= 12288 ? nlo + nhi : 0;
+}
+// shared memory of a COLPASS tile: sub-transform twiddles, four-step table, tile
+inline __host__ __device__ size_t cfft_colpass_smem(int twlen, int bits, int N, int tile_elems, int elem_bytes) {
+    const size_t a = ((size_t)cfft_pass_tw_elems(twlen, elem_bytes) * elem_bytes + 15) / 16 * 16;
+    return a + (size_t)cfft_pass_t4_elems(bits, N) * 16 + (size_t)tile_elems * elem_bytes + 16;
+}
 
 // One launch of the batched executor: parameter blocks in device memory and,
 // per block of the grid, the index of its parameter block.

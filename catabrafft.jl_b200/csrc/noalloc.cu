@@ -205,8 +205,8 @@ extern "C" int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, con
                 return noalloc_fail(CFFT_ERR_CUDA, "cudaGetSymbolAddress", ce);
             // shared-memory attributes for both element types' pass kernels
             for (int dt = 0; dt < 2 && ce == cudaSuccess; dt++) {
-                ce = cfft_prepare_fn(cfft_kernel_for(MODE_COLPASS, dt), 112 * 1024 + 16, 1);
-                if (ce == cudaSuccess) ce = cfft_prepare_fn(cfft_kernel_for(MODE_ROWPASS, dt), 112 * 1024 + 16, 1);
+                ce = cfft_prepare_fn(cfft_kernel_for(MODE_COLPASS, dt), 128 * 1024, 1);
+                if (ce == cudaSuccess) ce = cfft_prepare_fn(cfft_kernel_for(MODE_ROWPASS, dt), 128 * 1024, 1);
             }
             if (ce != cudaSuccess) return noalloc_fail(CFFT_ERR_CUDA, "kernel attributes", ce);
             g_arena_ptr[dev] = (unsigned char*)ptr;
@@ -273,7 +273,7 @@ extern "C" int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, con
     row.mV = magic(Vr);
     row.mN2 = magic(N2);
     row.post = POST_OUT;
-    const size_t smem_col = (size_t)(cfft_pass_tw_elems(pa.twlen, (int)e) + N1 * Vc) * e + 16;
+    const size_t smem_col = cfft_colpass_smem(pa.twlen, bits, (int)n, (int)(N1 * Vc), (int)e);
     const size_t smem_row = (size_t)(cfft_pass_tw_elems(pc.twlen, (int)e) + Vr * PC) * e + 16;
 
     const long long chunk = std::max<long long>(1, (long long)(kScratchBytes / ((size_t)n * e)));

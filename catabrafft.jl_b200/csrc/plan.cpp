@@ -901,8 +901,15 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         }
         return best2 ? best2 : best;
     };
+    // per-CTA budget: three ComplexF32 or two ComplexF64 CTAs per SM, the
+    // staged tables included
+    const size_t budget = (e == 8) ? 74 * 1024 : 112 * 1024;
     const size_t tile_lim = (e == 8) ? 72 * 1024 : 96 * 1024;
-    const int64_t Vc = pick_tile(N2, N1, tile_lim), Vr = pick_tile(N1, PC, tile_lim);
+    const size_t tabc = cfft_colpass_smem((int)twiddle_len(N1, sh.ra), twolevel_bits(M), (int)M, 0, (int)e);
+    const size_t tabr = (size_t)cfft_pass_tw_elems((int)twiddle_len(N2, sh.rc), (int)e) * e + 16;
+    const size_t lim_c = std::min(tile_lim, budget > tabc ? budget - tabc : 0);
+    const size_t lim_r = std::min(tile_lim, budget > tabr ? budget - tabr : 0);
+    const int64_t Vc = pick_tile(N2, N1, lim_c), Vr = pick_tile(N1, PC, lim_r);
     SubPlan pa, pc;
     rc = make_subplan(P, N1, sh.ra, Vc, pa, true);
     if (rc) return rc;
@@ -936,7 +943,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp.t4 = t4;
         s.kp.pre = pre;
         s.threads = CFFT_THREADS;
-        s.smem = (size_t)(cfft_pass_tw_elems(pa.twlen, (int)e) + N1 * Vc) * e + 16;
+        s.smem = cfft_colpass_smem(pa.twlen, t4.bits, t4.N, (int)(N1 * Vc), (int)e);
         s.cluster = 1;
         s.in_sel = in_sel;
         s.out_sel = out_sel;
