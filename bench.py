@@ -174,7 +174,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    budget = max(0.1, 60.0 / max(1, args.steps + args.warmup))   # the whole arm: about a minute
+    budget = max(0.05, args.ref_seconds / max(1, args.steps + args.warmup))   # the whole arm: about a minute
     cpu_reference(threads, 0.5, steps=max(0, min(args.warmup, 1)))
     res = cpu_reference(threads, budget, steps=args.steps)
     gbs = statistics.median(v for v, _, _ in res)
@@ -553,6 +553,8 @@ def main():
     ap.add_argument("--form", default="plain", choices=FORMS,
                     help="plain (the contract line) or one of the other workload forms")
     ap.add_argument("--count", type=int, default=20000, help="batch/serve form: transforms")
+    ap.add_argument("--ref-seconds", type=float, default=60.0,
+                    help="reference arm: CPU seconds spread over its warm-up and timed steps")
     args = ap.parse_args()
     global SIZES
     if args.only:
