@@ -318,7 +318,7 @@ def form_precision(torch, cb, lib, dev, args):
     """ComplexF32 arithmetic with FP64-generated twiddles: 4096 x 2^16 and
     4096 x 3^9, uniform(-1,1) parts; error vs this library's ComplexF64 path
     (itself held to 1e-12 of the oracle by the tests)."""
-    sizes = [(65536, 4096), (19683, 4096)]
+    sizes = [(65536, args.batch or 4096), (19683, args.batch or 4096)]
     g = torch.Generator(device=dev)
     g.manual_seed(11)
     st = torch.cuda.current_stream(dev)
