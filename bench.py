@@ -243,7 +243,7 @@ def measure_e2e(torch, cb, lib, plans, bufs, args, world, dev):
 
 
 # ---------------------------------------------------------------- other forms
-FORMS = ("plain", "small", "precision", "batch", "serve")
+FORMS = ("plain", "small", "precision", "pow2", "batch", "serve")
 
 
 def _setup_single():
@@ -372,6 +372,76 @@ def form_precision(torch, cb, lib, dev, args):
             "frac_of_hbm": round(v / peak, 4), "peak": peak, "peak_kind": kind, "dtype": "f32",
             "tolerance": 1e-5,
             "config": {"workload": "C64 4096 x 2^16 and 4096 x 3^9, uniform(-1,1), forward"}}
+
+
+def form_pow2(torch, cb, lib, dev, args):
+    """Plain ComplexF64 path on batched power-of-two lengths 2^12 .. 2^22,
+    1 GiB of input per size (beyond L2), iid N(0,1) parts; forward and
+    inverse per step.  GB/s against the HBM roofline and GFLOP/s in the
+    5 N log2 N convention, with torch.fft (cuFFT) on the same batch for
+    context."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(13)
+    st = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(st.cuda_stream)
+    vp = ctypes.c_void_p
+    peak, kind = load_peaks()
+    flag = {"none": cb.NO_FLAG, "measure": cb.MEASURE}[args.flag]
+    exps = [int(e) for e in args.exps.split(",")] if args.exps else list(range(12, 23))
+    out = {}
+    total_bytes, total_ms = 0, 0.0
+    for k in exps:
+        n = 1 << k
+        b = args.batch or max(1, (1 << 30) // (16 * n))
+        x = torch.complex(torch.randn(b, n, dtype=torch.float64, device=dev, generator=g),
+                          torch.randn(b, n, dtype=torch.float64, device=dev, generator=g))
+        y, z = torch.empty_like(x), torch.empty_like(x)
+        h = ctypes.c_void_p()
+        cb.check(lib.cfft_plan_create(ctypes.byref(h), n, b, cb.C128, flag))
+        for _ in range(max(3, args.warmup)):
+            lib.cfft_execute(h, vp(x.data_ptr()), vp(y.data_ptr()), 0, sp)
+            lib.cfft_execute(h, vp(y.data_ptr()), vp(z.data_ptr()), 1, sp)
+        steps = max(3, min(args.steps, 20))
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(steps):
+            lib.cfft_execute(h, vp(x.data_ptr()), vp(y.data_ptr()), 0, sp)
+            lib.cfft_execute(h, vp(y.data_ptr()), vp(z.data_ptr()), 1, sp)
+        e.record(st)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(e) / (2 * steps)
+        rt = (torch.linalg.norm(z - x) / torch.linalg.norm(x)).item()
+        desc = ctypes.create_string_buffer(256)
+        lib.cfft_plan_describe(h, desc, 256)
+        lib.cfft_plan_destroy(h)
+        # cuFFT on the same batch, forward only (context)
+        for _ in range(3):
+            torch.fft.fft(x, dim=1)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(steps):
+            torch.fft.fft(x, dim=1)
+        e.record(st)
+        torch.cuda.synchronize()
+        lib_ms = a.elapsed_time(e) / steps
+        nbytes = 2 * n * b * 16
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[str(n)] = {"batch": b, "ms_per_launch": round(ms, 4), "GB_s": round(gbs, 2),
+                       "frac_of_hbm": round(gbs / peak, 4),
+                       "GFLOP_s": round(5 * n * k * b / (ms * 1e-3) / 1e9, 1),
+                       "cufft_ms": round(lib_ms, 4), "roundtrip_rel_l2": rt, "plan": desc.value.decode()}
+        total_bytes += nbytes
+        total_ms += ms
+        del x, y, z
+        torch.cuda.empty_cache()
+    v = total_bytes / (total_ms * 1e-3) / 1e9
+    return {"form": "pow2", "metric": "FFT GB/s vs HBM peak, ComplexF64, batched power-of-two n",
+            "value": round(v, 2), "unit": "GB/s", "higher_is_better": True, "per_size": out,
+            "frac_of_hbm": round(v / peak, 4), "peak": peak, "peak_kind": kind, "dtype": "f64",
+            "plan_flag": args.flag,
+            "config": {"workload": "C128, n = 2^12 .. 2^22, 1 GiB of input per size, iid N(0,1), "
+                                   "forward + inverse; inputs larger than L2"}}
 
 
 def form_batch(torch, cb, lib, dev, args):
@@ -509,7 +579,7 @@ def run_form(args):
     if env is None:
         return 0
     torch, cb, lib, dev = env
-    fn = {"small": form_small, "precision": form_precision, "batch": form_batch,
+    fn = {"small": form_small, "precision": form_precision, "pow2": form_pow2, "batch": form_batch,
           "serve": form_serve}[args.form]
     line = fn(torch, cb, lib, dev, args)
     line.update({"n_gpus": 1, "warmup": args.warmup, "data": "synthetic (seeded)"})
@@ -553,6 +623,8 @@ def main():
     ap.add_argument("--form", default="plain", choices=FORMS,
                     help="plain (the contract line) or one of the other workload forms")
     ap.add_argument("--count", type=int, default=20000, help="batch/serve form: transforms")
+    ap.add_argument("--exps", default="", help="pow2 form: comma-separated log2 lengths (default 12..22)")
+    ap.add_argument("--flag", default="none", choices=("none", "measure"), help="pow2 form: plan flag")
     ap.add_argument("--ref-seconds", type=float, default=60.0,
                     help="reference arm: CPU seconds spread over its warm-up and timed steps")
     args = ap.parse_args()

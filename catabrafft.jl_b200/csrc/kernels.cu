@@ -130,6 +130,19 @@ cudaError_t cfft_launch_batch(const void* f, const BatchLaunch& L, unsigned grid
     return e;
 }
 
+// n = 4096: one transform per CTA, registers + two shared-memory exchanges
+template <typename V>
+__global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) k_r4096(KParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    r4096_body<V>(p, smem);
+}
+const void* cfft_r4096_kernel(int dtype) {
+    return dtype == CFFT_DT_C128 ? (const void*)k_r4096<double2> : (const void*)k_r4096<float2>;
+}
+size_t cfft_r4096_smem(size_t elem_bytes) {
+    return ((16 * R4096_PL * elem_bytes + 15) & ~(size_t)15) + 129 * sizeof(double2);
+}
+
 const void* cfft_kernel_for(int mode, int dtype) {
     if (dtype == CFFT_DT_C128) {
         switch (mode) {

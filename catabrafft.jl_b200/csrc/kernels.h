@@ -17,6 +17,10 @@ const void* cfft_kernel_for(int mode, int dtype);
 // nullptr; *single (if given) = 1 when it keeps one buffer for both layouts
 const void* cfft_static_four(int dtype, int N1, int N2, int C, const unsigned char* ca,
                              const unsigned char* cc, int* single = nullptr);
+// n = 4096 register kernel (KParams of a one-transform-per-CTA ROWS stage
+// plus t4 = the two-level table of w_4096) and its shared memory
+const void* cfft_r4096_kernel(int dtype);
+size_t cfft_r4096_smem(size_t elem_bytes);
 cudaError_t cfft_prepare_fn(const void* fn, size_t smem, int cluster);
 cudaError_t cfft_launch_fn(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
                            int cluster, cudaStream_t stream);

@@ -822,6 +822,16 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.in_sel = 0;
         s.out_sel = 1;
         s.fn = cfft_kernel_for(MODE_ROWS, P->dtype);
+        if (sh.conv == CONV_NONE && sh.M == 4096 && sh.V == 1) {
+            // the register kernel; descriptor-driven launches keep the
+            // generic rows kernel and its shared memory
+            rc = make_twolevel(P, 4096, s.kp.t4);
+            if (rc) return rc;
+            s.fn = cfft_r4096_kernel(P->dtype);
+            s.smem_batched = sh.smem;
+            s.smem = cfft_r4096_smem(elem_bytes(P->dtype));
+            P->desc += "+r4096";
+        }
         CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, 1));
         P->stages.push_back(s);
         P->chunk = P->batch;

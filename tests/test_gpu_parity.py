@@ -207,3 +207,32 @@ def test_empty_cache_releases_plans(cb):
     cb.fft(x)
     cb.empty_cache()
     assert rel(cb.fft(x)[:1], np.array([4096.0 + 0j])) < 1e-15
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, TOL64), (np.complex64, TOL32)])
+def test_register_kernel_n4096(cb, dtype, tol):
+    # n = 4096 runs the register kernel (16 x 16 x 16, one transform per CTA);
+    # forward / inverse / backward against the oracle, batched and single,
+    # in place, and through the descriptor-driven batch path
+    import torch
+    rng = np.random.default_rng(4096)
+    n = 4096
+    for batch in (1, 3, 300):
+        x = cplx(rng, (batch, n), dtype)
+        p = cb.plan_fft(x)
+        assert "+r4096" in p.describe(), p.describe()
+        xx = x.astype(np.complex128)
+        assert rel(cb.fft(x), oracle.fft(xx)) < tol
+        assert rel(cb.ifft(x), oracle.ifft(xx)) < tol
+        assert rel(cb.bfft(x), oracle.bfft(xx)) < tol
+    t = torch.from_numpy(x).cuda()
+    y = cb.fft(x)
+    cb.fft_(t)
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy(), y)
+    b = cb.Batch([n, 30240, n], dtype)
+    xb = cplx(rng, b.total, dtype)
+    yb = b.execute(torch.from_numpy(xb).cuda()).cpu().numpy()
+    for o, m in zip(b.offsets, [n, 30240, n]):
+        assert rel(yb[o:o + m], oracle.fft(xb[o:o + m].astype(np.complex128))) < tol, m
+    b.close()
