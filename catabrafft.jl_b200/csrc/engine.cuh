@@ -263,64 +263,82 @@ __device__ __forceinline__ double2 block_sum(double2 v, double2* scratch) {
 }
 
 // ------------------------------------------- n = 4096 held in registers
-// One 4096-point transform per CTA of 256 threads, 16 elements per thread,
+// 4096-point transforms on CTAs of 256 threads, 16 elements per thread,
 // as 4096 = 16 x 256 and 256 = 16 x 16 (three radix-16 stages):
-//   A: thread t loads x[t + 256 k] (k < 16) straight from HBM (each k is one
-//      coalesced row of the transform), DFT_16 over k, twiddle w_4096^(t k1),
-//      stores Y[k1][t] to shared memory;
+//   A: thread t takes x[t + 256 k] (k < 16; each k is one coalesced row of
+//      the transform, copied from HBM by cp.async), DFT_16 over k, twiddle
+//      w_4096^(t k1), stores Y[k1][t] to shared memory;
 //   B: thread (t1, k1) = (t & 15, t >> 4) reads Y[k1][t1 + 16 t2], DFT_16
 //      over t2, twiddle w_256^(t1 k2) = w_4096^(16 t1 k2), stores
 //      Z[k1][k2][t1] at k1*273 + k2*17 + t1;
 //   C: thread (k1, k2) = (t & 15, t >> 4) reads Z[k1][k2][t1], DFT_16 over
 //      t1 and stores X[k1 + 16 k2 + 256 k3] = X[t + 256 k3] straight to HBM.
-// Two shared-memory exchanges replace the generic path's staging copy and
-// three in-place passes.  Every shared access is conflict-free: 16-byte
+// Two shared-memory exchanges replace the generic path's three in-place
+// passes.  Every shared access is conflict-free: 16-byte
 // accesses are served a quarter-warp and 8-byte ones a half-warp at a time,
 // and within one of those groups the addresses run with stride 1 or 273
 // (odd), so they fall in distinct bank groups.  The FP64 two-level twiddle
 // table (w_4096^e = lo[e & 63] hi[e >> 6]) is staged in shared memory.
 constexpr int R4096_PB = 17, R4096_PL = 273;
+// Persistent: CTA g transforms g, g + gridDim.x, ...  A thread's input
+// elements x[t + 256 k] are copied by cp.async to buf[t + 256 k], exactly
+// where the same thread later reads them and writes its Y values, so the
+// input needs no block barrier.  The next transform's input is issued as soon
+// as every thread has read Z (the buffer is free), and lands while stage C
+// computes and stores and while the co-resident CTA works.
+template <typename V>
+__device__ __forceinline__ void r4096_prefetch(const KParams& p, V* buf, int b, int t) {
+    const V* in = (const V*)p.in + (long long)b * p.in_dist;
+#pragma unroll
+    for (int k = 0; k < 16; k++) cp_async_elem(buf + t + 256 * k, in + t + 256 * k);
+}
 template <typename V>
 __device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem) {
     V* buf = (V*)smem;                          // 16 planes of R4096_PL elements
     double2* tlo = after16(buf + 16 * R4096_PL);
     double2* thi = tlo + 64;
-    const int b = block_id(p);
-    if (b >= p.batch) return;                   // uniform across the CTA
     const int t = opaque_tid();
-    const V* in = (const V*)p.in + (long long)b * p.in_dist;
-    V* out = (V*)p.out + (long long)b * p.out_dist;
-    V v[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) v[k] = ldg_stream(in + t + 256 * k);
+    int b = block_id(p);
+    if (b >= p.batch) return;                   // uniform across the CTA
+    r4096_prefetch(p, buf, b, t);
+    cp_async_commit();
     if (t < 64) tlo[t] = p.t4.lo[t];
     if (t < 65) thi[t] = p.t4.hi[t];
     TwoLevel tw = p.t4;
     tw.lo = tlo;
     tw.hi = thi;
-#pragma unroll
-    for (int k = 0; k < 16; k++) v[k] = load_in(p, v[k]);
-    dft<16>(v);
     __syncthreads();                            // tables staged
+    for (; b < p.batch; b += gridDim.x) {
+        V v[16];
+        cp_async_wait_all();                    // this thread's own input elements
 #pragma unroll
-    for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = apply_tw(v[k1], tw, (unsigned)(t * k1));
-    __syncthreads();
-    {
-        const int t1 = t & 15, k1 = t >> 4;
-#pragma unroll
-        for (int t2 = 0; t2 < 16; t2++) v[t2] = buf[k1 * 256 + t1 + 16 * t2];
+        for (int k = 0; k < 16; k++) v[k] = load_in(p, buf[t + 256 * k]);
         dft<16>(v);
-        __syncthreads();                        // every Y read before Z overwrites it
 #pragma unroll
-        for (int k2 = 0; k2 < 16; k2++)
-            buf[k1 * R4096_PL + k2 * R4096_PB + t1] = apply_tw(v[k2], tw, (unsigned)(16 * t1 * k2));
-    }
-    __syncthreads();
-    {
-        const int k1 = t & 15, k2 = t >> 4;
+        for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = apply_tw(v[k1], tw, (unsigned)(t * k1));
+        __syncthreads();
+        {
+            const int t1 = t & 15, k1 = t >> 4;
 #pragma unroll
-        for (int t1 = 0; t1 < 16; t1++) v[t1] = buf[k1 * R4096_PL + k2 * R4096_PB + t1];
+            for (int t2 = 0; t2 < 16; t2++) v[t2] = buf[k1 * 256 + t1 + 16 * t2];
+            dft<16>(v);
+            __syncthreads();                    // every Y read before Z overwrites it
+#pragma unroll
+            for (int k2 = 0; k2 < 16; k2++)
+                buf[k1 * R4096_PL + k2 * R4096_PB + t1] = apply_tw(v[k2], tw, (unsigned)(16 * t1 * k2));
+        }
+        __syncthreads();
+        {
+            const int k1 = t & 15, k2 = t >> 4;
+#pragma unroll
+            for (int t1 = 0; t1 < 16; t1++) v[t1] = buf[k1 * R4096_PL + k2 * R4096_PB + t1];
+        }
+        __syncthreads();                        // every Z read: the buffer is free
+        const int bn = b + (int)gridDim.x;
+        if (bn < p.batch) r4096_prefetch(p, buf, bn, t);
+        cp_async_commit();
         dft<16>(v);
+        V* out = (V*)p.out + (long long)b * p.out_dist;
 #pragma unroll
         for (int k3 = 0; k3 < 16; k3++) stg_stream(out + t + 256 * k3, store_out(p, v[k3]));
     }

@@ -229,6 +229,7 @@ struct Stage {
     int in_sel, out_sel;     // 0 user in, 1 user out, 2 scratch0, 3 scratch1
     int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
     size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
+    unsigned persist = 0;    // kernels that loop over the batch: CTAs to launch at most
 };
 
 struct Shape {
@@ -458,11 +459,13 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
         for (int tries = 0; tries < 256; tries++) {
             if (global_shape(M2, dtype, g)) {
                 g.conv = c2;
-                // measured on B200: for ComplexF32 transforms of 2^15 points
-                // and more the two passes beat a cluster (1.3-1.5x at
-                // 2^16-2^17); otherwise second in line, so the heuristic
-                // keeps a single-kernel shape and MEASURE/ENCHANT time both
-                const bool first = dtype == CFFT_C64 && conv == CONV_NONE && M >= 32768;
+                // measured on B200: from 2^15 points the two passes beat a
+                // cluster for ComplexF32 transforms (1.3-1.5x at 2^16-2^17)
+                // and for power-of-two ComplexF64 ones (1.3x at 2^15, 1.7x
+                // at 2^16); otherwise second in line, so the heuristic keeps
+                // a single-kernel shape and MEASURE/ENCHANT time both
+                const bool pow2 = (M & (M - 1)) == 0;
+                const bool first = (dtype == CFFT_C64 || pow2) && conv == CONV_NONE && M >= 32768;
                 v.insert(v.begin() + (first ? 0 : std::min<size_t>(v.size(), 1)), g);
                 break;
             }
@@ -833,6 +836,13 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
             P->desc += "+r4096";
         }
         CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, 1));
+        if (s.fn == cfft_r4096_kernel(P->dtype)) {
+            // persistent: as many CTAs as are co-resident
+            int nsm = 0, occ = 0;
+            CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P->device));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s.fn, CFFT_THREADS, s.smem));
+            s.persist = (unsigned)(std::max(1, occ) * std::max(1, nsm));
+        }
         P->stages.push_back(s);
         P->chunk = P->batch;
         return CFFT_OK;
@@ -1049,6 +1059,7 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             else if (kp.mode == MODE_FOUR) grid = (unsigned)(nb * kp.C);
             else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
             else grid = (unsigned)(nb * (kp.N1 / kp.V));
+            if (s.persist && grid > s.persist) grid = s.persist;
             cudaError_t ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             if (ce != cudaSuccess)
                 return fail(CFFT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));

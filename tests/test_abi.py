@@ -77,6 +77,7 @@ def test_python_api_argument_errors():
     (1, "rows"), (4096, "rows(V=1)[16,16,16]"), (30240, "four(C="), (10007, "rader(n=10007,M=20160)+four"),
     (89, "rader(n=89,M=175)+rows"), (10006, "bluestein(n=10006,M=20160)"),
     (2 ** 20, "twopass(N1=1024,N2=1024)"), (2 ** 22, "twopass(N1=2048,N2=2048)"),
+    (2 ** 15, "twopass(N1=128,N2=256)"), (2 ** 16, "twopass(N1=256,N2=256)"), (60480, "four(C="),
 ])
 def test_strategy_choice(n, expect):
     m = load()
