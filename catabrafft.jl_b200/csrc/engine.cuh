@@ -278,8 +278,20 @@ __device__ __forceinline__ double2 block_sum(double2 v, double2* scratch) {
 // accesses are served a quarter-warp and 8-byte ones a half-warp at a time,
 // and within one of those groups the addresses run with stride 1 or 273
 // (odd), so they fall in distinct bank groups.  The FP64 two-level twiddle
-// table (w_4096^e = lo[e & 63] hi[e >> 6]) is staged in shared memory.
+// table (w_4096^e = lo[e & 63] hi[e >> 6]) is staged in shared memory, lo
+// entry l at l ^ (l >> 3): the exponents t k1 and 16 t1 k2 of a quarter-warp
+// step by multiples of 2, 8 or 16, which in natural order land in the same
+// bank group.
 constexpr int R4096_PB = 17, R4096_PL = 273;
+__device__ __forceinline__ double2 r4096_w(const double2* lo, const double2* hi, unsigned e) {
+    const unsigned l = e & 63;
+    return cmul(lo[l ^ (l >> 3)], hi[e >> 6]);
+}
+// x w_4096^e, the twiddle evaluated in FP64 and rounded once to V
+template <typename V>
+__device__ __forceinline__ V r4096_tw(V v, const double2* lo, const double2* hi, unsigned e) {
+    return e ? cmul(v, fromd<V>(r4096_w(lo, hi, e))) : v;
+}
 // Persistent: CTA g transforms g, g + gridDim.x, ...  A thread's input
 // elements x[t + 256 k] are copied by cp.async to buf[t + 256 k], exactly
 // where the same thread later reads them and writes its Y values, so the
@@ -297,25 +309,27 @@ __device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem
     V* buf = (V*)smem;                          // 16 planes of R4096_PL elements
     double2* tlo = after16(buf + 16 * R4096_PL);
     double2* thi = tlo + 64;
-    const int t = opaque_tid();
     int b = block_id(p);
     if (b >= p.batch) return;                   // uniform across the CTA
-    r4096_prefetch(p, buf, b, t);
-    cp_async_commit();
-    if (t < 64) tlo[t] = p.t4.lo[t];
-    if (t < 65) thi[t] = p.t4.hi[t];
-    TwoLevel tw = p.t4;
-    tw.lo = tlo;
-    tw.hi = thi;
+    {
+        const int t = opaque_tid();
+        r4096_prefetch(p, buf, b, t);
+        cp_async_commit();
+        if (t < 64) tlo[t ^ (t >> 3)] = p.t4.lo[t];
+        if (t < 65) thi[t] = p.t4.hi[t];
+    }
     __syncthreads();                            // tables staged
     for (; b < p.batch; b += gridDim.x) {
+        // re-read per transform: index math hoisted out of the loop would
+        // stay live across it and push the FP64 codelets into spills
+        const int t = opaque_tid();
         V v[16];
         cp_async_wait_all();                    // this thread's own input elements
 #pragma unroll
         for (int k = 0; k < 16; k++) v[k] = load_in(p, buf[t + 256 * k]);
         dft<16>(v);
 #pragma unroll
-        for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = apply_tw(v[k1], tw, (unsigned)(t * k1));
+        for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = r4096_tw(v[k1], tlo, thi, (unsigned)(t * k1));
         __syncthreads();
         {
             const int t1 = t & 15, k1 = t >> 4;
@@ -325,7 +339,7 @@ __device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem
             __syncthreads();                    // every Y read before Z overwrites it
 #pragma unroll
             for (int k2 = 0; k2 < 16; k2++)
-                buf[k1 * R4096_PL + k2 * R4096_PB + t1] = apply_tw(v[k2], tw, (unsigned)(16 * t1 * k2));
+                buf[k1 * R4096_PL + k2 * R4096_PB + t1] = r4096_tw(v[k2], tlo, thi, (unsigned)(16 * t1 * k2));
         }
         __syncthreads();
         {

@@ -131,7 +131,7 @@ cudaError_t cfft_launch_batch(const void* f, const BatchLaunch& L, unsigned grid
 }
 
 // n = 4096: persistent CTAs, registers + two shared-memory exchanges.  Three
-// CTAs per SM (80 registers; ComplexF64 spills 24 bytes) measured 2 % faster
+// CTAs per SM (80 registers; a few dozen bytes of spills) measured faster
 // than two without spills: more transforms in flight hide the HBM latency.
 template <typename V>
 __global__ void __launch_bounds__(CFFT_THREADS, 3) k_r4096(KParams p) {
