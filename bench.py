@@ -29,6 +29,18 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_package():
+    """The product package, through its own by-path loader."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "catabra_b200_load", os.path.join(ROOT, "catabrafft.jl_b200", "_load.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m.load()
+
+
 SIZES = [(30240, 1024), (10007, 1024)]
 ELEM = 16  # ComplexF64 bytes
 METRIC = "FFT GB/s vs HBM peak, plain vs batched/served; p50/p99 latency at stated err"
@@ -252,9 +264,7 @@ def _setup_single():
     if rank != 0:
         return None
     torch.cuda.set_device(local)
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from _pkg import load
-    cb = load()
+    cb = load_package()
     return torch, cb, cb._lib.LIB, torch.device("cuda", local)
 
 
@@ -412,6 +422,12 @@ def form_pow2(torch, cb, lib, dev, args):
         torch.cuda.synchronize()
         ms = a.elapsed_time(e) / (2 * steps)
         rt = (torch.linalg.norm(z - x) / torch.linalg.norm(x)).item()
+        # correctness gate at the measured batch: the round trip, and the
+        # forward transform of the first and last rows against cuFFT (a
+        # forward-only error would cancel in the round trip)
+        ref = torch.fft.fft(x[[0, b - 1]], dim=1)
+        fwd_err = (torch.linalg.norm(y[[0, b - 1]] - ref) / torch.linalg.norm(ref)).item()
+        assert rt < 1e-12 and fwd_err < 1e-12, (n, rt, fwd_err)
         desc = ctypes.create_string_buffer(256)
         lib.cfft_plan_describe(h, desc, 256)
         lib.cfft_plan_destroy(h)
@@ -430,7 +446,8 @@ def form_pow2(torch, cb, lib, dev, args):
         out[str(n)] = {"batch": b, "ms_per_launch": round(ms, 4), "GB_s": round(gbs, 2),
                        "frac_of_hbm": round(gbs / peak, 4),
                        "GFLOP_s": round(5 * n * k * b / (ms * 1e-3) / 1e9, 1),
-                       "cufft_ms": round(lib_ms, 4), "roundtrip_rel_l2": rt, "plan": desc.value.decode()}
+                       "cufft_ms": round(lib_ms, 4), "roundtrip_rel_l2": rt, "fwd_rel_l2_vs_cufft": fwd_err,
+                       "plan": desc.value.decode()}
         total_bytes += nbytes
         total_ms += ms
         del x, y, z
@@ -647,9 +664,7 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from _pkg import load
-    cb = load()
+    cb = load_package()
     lib = cb._lib.LIB
 
     g = torch.Generator(device=dev)

@@ -56,6 +56,7 @@ SIGNATURES = {
     "cfft_wisdom_import": (_ci, [_cp]),
     "cfft_wisdom_forget": (_ci, []),
     "cfft_wisdom_entries": (_i64, []),
+    "cfft_debug_alloc_hook": (_i64, [_i64]),
 }
 
 

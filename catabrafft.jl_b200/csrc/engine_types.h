@@ -89,6 +89,35 @@ inline __host__ __device__ size_t cfft_colpass_smem(int twlen, int bits, int N, 
     return a + (size_t)cfft_pass_t4_elems(bits, N) * 16 + (size_t)tile_elems * elem_bytes + 16;
 }
 
+// Tile widths of the two pass kernels for M = N1 x N2 (host side; the
+// planner and the no-allocation entry point use the same rule).  A width is a
+// divisor of the tile count of at most 64 whose tile fits the per-CTA budget
+// (three ComplexF32 or two ComplexF64 CTAs per SM, staged tables included);
+// a power of two whose V-element global segments span at least 128 bytes is
+// preferred (it divides the block, so each thread keeps one column in the
+// column pass's epilogue), else the widest that fits.
+inline long long cfft_pick_tile(long long count, long long per, size_t limit, size_t e) {
+    long long best = 1, best2 = 0;
+    for (long long v = 1; v <= count && v <= 64; v++) {
+        if (count % v || (size_t)(v * per) * e > limit) continue;
+        best = v;
+        if ((v & (v - 1)) == 0 && (size_t)v * e >= 128) best2 = v;
+    }
+    return best2 ? best2 : best;
+}
+// *Vc: columns per COLPASS tile; *Vr: rows per ROWPASS tile (row pitch PC)
+inline void cfft_pass_tiles(long long N1, long long N2, long long PC, int twA, int twC, int bits, int M,
+                            size_t e, long long* Vc, long long* Vr) {
+    const size_t budget = (e == 8) ? 74 * 1024 : 112 * 1024;
+    const size_t tile_lim = (e == 8) ? 72 * 1024 : 96 * 1024;
+    const size_t tabc = cfft_colpass_smem(twA, bits, M, 0, (int)e);
+    const size_t tabr = (size_t)cfft_pass_tw_elems(twC, (int)e) * e + 16;
+    const size_t room_c = budget > tabc ? budget - tabc : 0, room_r = budget > tabr ? budget - tabr : 0;
+    const size_t lim_c = room_c < tile_lim ? room_c : tile_lim, lim_r = room_r < tile_lim ? room_r : tile_lim;
+    *Vc = cfft_pick_tile(N2, N1, lim_c, e);
+    *Vr = cfft_pick_tile(N1, PC, lim_r, e);
+}
+
 // One launch of the batched executor: parameter blocks in device memory and,
 // per block of the grid, the index of its parameter block.
 struct BatchLaunch {

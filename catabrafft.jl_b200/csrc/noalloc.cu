@@ -2,13 +2,13 @@
 // device allocation.
 //
 // Some callers cannot allocate device memory at the moment they need a
-// transform: code running inside a pool that forbids cudaMalloc, inside a
-// framework that owns every allocation through its own allocator, or while
-// a stream is being captured into a CUDA graph (where cudaMalloc is not a
-// capturable operation).  This entry point serves them: its scratch (the
-// intermediate between the column pass and the row pass) and its twiddle
-// tables live in one file-scope __device__ array of fixed size that every GPU
-// loading the library holds until the process exits.  The caller passes the
+// transform: code running inside a memory pool that forbids cudaMalloc, or
+// inside a framework that owns every allocation through its own allocator
+// and may not see the library allocate behind its back.  This entry point
+// serves them: its scratch (the intermediate between the column pass and the
+// row pass) and its twiddle tables live in one file-scope __device__ array of
+// fixed size that every GPU loading the library holds until the process
+// exits.  The caller passes the
 // input and output; nothing else is allocated -- no cudaMalloc / cudaFree,
 // no allocating library call, no host heap.
 //
@@ -18,8 +18,9 @@
 //     elements); larger or non-smooth n are rejected with CFFT_ERR_UNSUPPORTED.
 //   * The batch is processed in chunks that fit the scratch.
 //   * The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) and sets kernel attributes; make that first call
-//     before any stream capture begins.
+//     (cudaGetSymbolAddress) and sets kernel attributes, once per device,
+//     with that device current; make that first call before any stream
+//     capture begins.
 //   * Every call shares the array, and each call overwrites the tables and
 //     scratch it uses (nothing is assumed to start at zero): calls that
 //     overlap on the GPU -- on different streams, or from different host
@@ -147,13 +148,6 @@ void pass_table(const SubPlan& sp, PassTable& T) {
 unsigned long long magic(long long d) {
     return ((1ULL << 40) + (unsigned long long)d - 1) / (unsigned long long)d;
 }
-int largest_tile(long long count, long long per, size_t e) {
-    int best = 1;
-    for (long long v = 1; v <= count && v <= 64; v++)
-        if (count % v == 0 && (size_t)(v * per) * e <= 96 * 1024) best = (int)v;
-    return best;
-}
-
 }  // namespace
 
 extern "C" int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, const void* d_in,
@@ -258,16 +252,19 @@ extern "C" int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, con
     pa.tw = twA;
     pc.tw = twC;
     const long long PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
-    const int Vc = largest_tile(N2, N1, e), Vr = largest_tile(N1, PC, e);
+    // the planner's tile rule: widths within the per-CTA shared-memory budget
+    // (staged tables included), power-of-two widths preferred
+    long long Vc = 1, Vr = 1;
+    cfft_pass_tiles(N1, N2, PC, pa.twlen, pc.twlen, bits, (int)n, e, &Vc, &Vr);
     KParams col = kp, row = kp;
     col.mode = MODE_COLPASS;
-    col.V = Vc;
-    col.PA = Vc;
+    col.V = (int)Vc;
+    col.PA = (int)Vc;
     col.pa = pa;
     col.mV = magic(Vc);
     col.pre = PRE_NONE;
     row.mode = MODE_ROWPASS;
-    row.V = Vr;
+    row.V = (int)Vr;
     row.PC = (int)PC;
     row.pc = pc;
     row.mV = magic(Vr);

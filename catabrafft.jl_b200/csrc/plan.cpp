@@ -40,6 +40,47 @@ static int fail(int code, const std::string& msg) {
     cfft_set_last_error(msg.c_str());
     return code;
 }
+// ------------------------------------------------- allocation accounting
+// Every device and pinned-host allocation of the library goes through these
+// wrappers: they count live allocations and, for tests of the failure paths,
+// can make allocations fail as out of memory (cfft_debug_alloc_hook).
+static std::atomic<int64_t> g_live_allocs{0};
+static std::atomic<int64_t> g_alloc_seq{0};       // allocations since the hook was last set
+static std::atomic<int64_t> g_alloc_fail_from{0}; // 0: off; else fail the nth and later
+static bool alloc_injected_failure() {
+    const int64_t from = g_alloc_fail_from.load();
+    if (from <= 0) return false;
+    return g_alloc_seq.fetch_add(1) + 1 >= from;
+}
+template <class T> static cudaError_t lib_malloc(T** p, size_t bytes) {
+    if (alloc_injected_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e == cudaSuccess) g_live_allocs.fetch_add(1);
+    return e;
+}
+template <class T> static cudaError_t lib_host_alloc(T** p, size_t bytes, unsigned flags) {
+    if (alloc_injected_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    cudaError_t e = cudaHostAlloc((void**)p, bytes, flags);
+    if (e == cudaSuccess) g_live_allocs.fetch_add(1);
+    return e;
+}
+static cudaError_t lib_free(void* p) {
+    if (!p) return cudaSuccess;
+    g_live_allocs.fetch_sub(1);
+    return cudaFree(p);
+}
+static cudaError_t lib_free_host(void* p) {
+    if (!p) return cudaSuccess;
+    g_live_allocs.fetch_sub(1);
+    return cudaFreeHost(p);
+}
+
 #define CUDA_TRY(call)                                                                     \
     do {                                                                                   \
         cudaError_t e_ = (call);                                                           \
@@ -251,7 +292,7 @@ struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) lib_free(p);
     }
 };
 using DevPtr = std::shared_ptr<DevBuf>;
@@ -275,7 +316,7 @@ struct cfft_plan_s {
     int64_t host_chunk = 0;
     void* host_buf[3] = {nullptr, nullptr, nullptr};
     cudaStream_t host_st[3] = {nullptr, nullptr, nullptr};   // in, compute, out
-    cudaEvent_t ev_in[3], ev_comp[3], ev_out[3];
+    cudaEvent_t ev_in[3] = {}, ev_comp[3] = {}, ev_out[3] = {};
     void* stage_in[3] = {nullptr, nullptr, nullptr};    // pinned staging for pageable callers
     void* stage_out[3] = {nullptr, nullptr, nullptr};
     // strided plans (cfft_plan_create_many): element i of transform b at
@@ -490,7 +531,7 @@ static std::string shape_desc(const Shape& s, int64_t n) {
 
 // ---------------------------------------------------------- device tables
 static int dev_upload(cfft_plan_s* P, const void* h, size_t bytes, void** d) {
-    CUDA_TRY(cudaMalloc(d, bytes));
+    CUDA_TRY(lib_malloc(d, bytes));
     P->allocs.push_back(*d);
     CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
     return CFFT_OK;
@@ -500,7 +541,7 @@ static std::map<std::string, DevPtr> g_tables;
 
 static int dev_alloc(size_t bytes, DevPtr* out) {
     auto b = std::make_shared<DevBuf>();
-    cudaError_t e = cudaMalloc(&b->p, bytes);
+    cudaError_t e = lib_malloc(&b->p, bytes);
     if (e != cudaSuccess) {
         b->p = nullptr;
         cudaGetLastError();
@@ -908,28 +949,14 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     // two HBM passes per FFT_M (and two FFT_M for a convolution)
     const int64_t N1 = sh.N1, N2 = sh.N2, M = sh.M;
     const int64_t PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
-    // tile width V: a divisor of the tile count; prefer a power of two (it
-    // divides the block, so each thread keeps one column in the epilogue)
-    // whose V-element global segments span at least 128 bytes, else the
-    // widest that fits.  ComplexF32 pass kernels run three CTAs per SM.
-    auto pick_tile = [&](int64_t count, int64_t per, size_t limit) {
-        int64_t best = 1, best2 = 0;
-        for (int64_t v = 1; v <= count; v++) {
-            if (count % v || (size_t)(v * per) * e > limit || v > 64) continue;
-            best = v;
-            if ((v & (v - 1)) == 0 && (size_t)v * e >= 128) best2 = v;
-        }
-        return best2 ? best2 : best;
-    };
-    // per-CTA budget: three ComplexF32 or two ComplexF64 CTAs per SM, the
-    // staged tables included
-    const size_t budget = (e == 8) ? 74 * 1024 : 112 * 1024;
-    const size_t tile_lim = (e == 8) ? 72 * 1024 : 96 * 1024;
-    const size_t tabc = cfft_colpass_smem((int)twiddle_len(N1, sh.ra), twolevel_bits(M), (int)M, 0, (int)e);
-    const size_t tabr = (size_t)cfft_pass_tw_elems((int)twiddle_len(N2, sh.rc), (int)e) * e + 16;
-    const size_t lim_c = std::min(tile_lim, budget > tabc ? budget - tabc : 0);
-    const size_t lim_r = std::min(tile_lim, budget > tabr ? budget - tabr : 0);
-    const int64_t Vc = pick_tile(N2, N1, lim_c), Vr = pick_tile(N1, PC, lim_r);
+    int64_t Vc = 1, Vr = 1;
+    {
+        long long vc = 1, vr = 1;
+        cfft_pass_tiles(N1, N2, PC, (int)twiddle_len(N1, sh.ra), (int)twiddle_len(N2, sh.rc), twolevel_bits(M),
+                        (int)M, e, &vc, &vr);
+        Vc = vc;
+        Vr = vr;
+    }
     SubPlan pa, pc;
     rc = make_subplan(P, N1, sh.ra, Vc, pa, true);
     if (rc) return rc;
@@ -946,7 +973,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     P->scratch_bytes = (size_t)chunk * M * e;
     if (!P->shared_scratch) {
         for (int i = 0; i < nscr; i++) {
-            CUDA_TRY(cudaMalloc(&P->scratch[i], P->scratch_bytes));
+            CUDA_TRY(lib_malloc(&P->scratch[i], P->scratch_bytes));
             P->allocs.push_back(P->scratch[i]);
         }
     }
@@ -1004,22 +1031,28 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     return CFFT_OK;
 }
 
-static void plan_free(cfft_plan_s* P) {
-    if (P->host_ready) {
-        for (int i = 0; i < 3; i++) {
-            cudaFree(P->host_buf[i]);
-            cudaStreamDestroy(P->host_st[i]);
-            cudaEventDestroy(P->ev_in[i]);
-            cudaEventDestroy(P->ev_comp[i]);
-            cudaEventDestroy(P->ev_out[i]);
-            P->host_buf[i] = nullptr;
-            if (P->stage_in[i]) cudaFreeHost(P->stage_in[i]);
-            if (P->stage_out[i]) cudaFreeHost(P->stage_out[i]);
-            P->stage_in[i] = P->stage_out[i] = nullptr;
-        }
-        P->host_ready = false;
+// the host entry's pipeline (device chunk buffers, streams, events, pinned
+// staging), whatever part of it exists
+static void host_release(cfft_plan_s* P) {
+    for (int i = 0; i < 3; i++) {
+        lib_free(P->host_buf[i]);
+        P->host_buf[i] = nullptr;
+        if (P->host_st[i]) cudaStreamDestroy(P->host_st[i]);
+        if (P->ev_in[i]) cudaEventDestroy(P->ev_in[i]);
+        if (P->ev_comp[i]) cudaEventDestroy(P->ev_comp[i]);
+        if (P->ev_out[i]) cudaEventDestroy(P->ev_out[i]);
+        P->host_st[i] = nullptr;
+        P->ev_in[i] = P->ev_comp[i] = P->ev_out[i] = nullptr;
+        lib_free_host(P->stage_in[i]);
+        lib_free_host(P->stage_out[i]);
+        P->stage_in[i] = P->stage_out[i] = nullptr;
     }
-    for (void* p : P->allocs) cudaFree(p);
+    P->host_ready = false;
+}
+
+static void plan_free(cfft_plan_s* P) {
+    host_release(P);
+    for (void* p : P->allocs) lib_free(p);
     P->allocs.clear();
     P->tables.clear();
     P->stages.clear();
@@ -1135,7 +1168,7 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
         cfft_plan_s* P = *out;
         P->io_half = true;
         P->desc = "f16io+" + P->desc;
-        if (cudaMalloc(&P->half_work, (size_t)n * batch * sizeof(float2)) != cudaSuccess) {
+        if (lib_malloc(&P->half_work, (size_t)n * batch * sizeof(float2)) != cudaSuccess) {
             cudaGetLastError();
             plan_free(P);
             delete P;
@@ -1161,11 +1194,19 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
     cudaGetDevice(&P->device);
     int rc = CFFT_ERR_UNSUPPORTED;
     if (level == CFFT_NO_FLAG) {
+        int nomem = 0;
+        std::string nomem_err;
         for (auto& c : cands) {
             rc = plan_build(P, c);
             if (rc == CFFT_OK) break;
+            if (rc == CFFT_ERR_NOMEM && !nomem) {
+                nomem = 1;
+                nomem_err = g_err;
+            }
             plan_free(P);
         }
+        // an out-of-memory failure outranks a later shape the device rejects
+        if (rc != CFFT_OK && nomem) rc = fail(CFFT_ERR_NOMEM, nomem_err);
     } else {
         const WisdomKey wk{n, batch, dtype, flags};
         std::string sig;
@@ -1186,30 +1227,40 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
         limit = std::min<size_t>(limit, 24);
         const size_t e = elem_bytes(dtype);
         void* buf = nullptr;
-        if (cudaMalloc(&buf, (size_t)n * batch * e) != cudaSuccess) {
+        if (lib_malloc(&buf, (size_t)n * batch * e) != cudaSuccess) {
             delete P;
             return fail(CFFT_ERR_NOMEM, "autotune buffer allocation failed");
         }
         cudaMemset(buf, 0, (size_t)n * batch * e);
         float best = 1e30f;
-        int best_i = -1;
+        int best_i = -1, cand_rc = CFFT_ERR_UNSUPPORTED;
         const char* logenv = getenv("CFFT_TUNE_LOG");      // diagnostics: one line per candidate
         const bool log = logenv && logenv[0] == '1';
+        std::string cand_err;
         for (size_t i = 0; i < limit; i++) {
-            if (plan_build(P, cands[i]) == CFFT_OK) {
+            const int brc = plan_build(P, cands[i]);
+            if (brc == CFFT_OK) {
                 float t = time_plan(P, buf);
                 if (log)
                     fprintf(stderr, "cfft-tune n=%lld batch=%lld %s smem=%zu co-resident=%d %.4f ms\n",
                             (long long)n, (long long)batch, P->desc.c_str(), P->stages[0].smem,
                             P->stages[0].max_units, t);
                 if (t < best) { best = t; best_i = (int)i; }
-            } else if (log) {
-                fprintf(stderr, "cfft-tune n=%lld candidate %zu failed: %s\n", (long long)n, i, g_err);
+            } else {
+                // an out-of-memory failure outranks a shape the device rejects
+                if (cand_rc != CFFT_ERR_NOMEM) {
+                    cand_rc = brc;
+                    cand_err = g_err;
+                }
+                if (log) fprintf(stderr, "cfft-tune n=%lld candidate %zu failed: %s\n", (long long)n, i, g_err);
             }
             plan_free(P);
         }
-        cudaFree(buf);
-        if (best_i < 0) { delete P; return fail(CFFT_ERR_UNSUPPORTED, "no candidate plan ran"); }
+        lib_free(buf);
+        if (best_i < 0) {
+            delete P;
+            return fail(cand_rc, "no candidate plan ran: " + cand_err);
+        }
         rc = plan_build(P, cands[best_i]);
         if (rc == CFFT_OK) wisdom_store(wk, shape_signature(cands[best_i]));
     }
@@ -1273,7 +1324,7 @@ static void batch_free(cfft_batch_s* B) {
         delete kv.second;
     }
     B->plans.clear();
-    for (void* q : B->allocs) cudaFree(q);
+    for (void* q : B->allocs) lib_free(q);
     B->allocs.clear();
 }
 
@@ -1351,9 +1402,9 @@ static int make_group(cfft_batch_s* B, const void* fn, int cluster, std::vector<
     g.ndesc = (int)desc.size();
     g.grid = (unsigned)map.size();
     void *dd = nullptr, *dm = nullptr;
-    CUDA_TRY(cudaMalloc(&dd, desc.size() * sizeof(KParams)));
+    CUDA_TRY(lib_malloc(&dd, desc.size() * sizeof(KParams)));
     B->allocs.push_back(dd);
-    CUDA_TRY(cudaMalloc(&dm, map.size() * sizeof(int)));
+    CUDA_TRY(lib_malloc(&dm, map.size() * sizeof(int)));
     B->allocs.push_back(dm);
     CUDA_TRY(cudaMemcpy(dd, desc.data(), desc.size() * sizeof(KParams), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(dm, map.data(), map.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1430,7 +1481,7 @@ static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* leng
             need_max = std::max(need_max, (size_t)P->shape.M * e * (P->stages.size() > 2 ? 2 : 1));
         }
         budget = std::max(budget, need_max);
-        CUDA_TRY(cudaMalloc(&B->scratch[0], budget));
+        CUDA_TRY(lib_malloc(&B->scratch[0], budget));
         B->allocs.push_back(B->scratch[0]);
         size_t used = 0;
         std::vector<int64_t> chunk;
@@ -1710,13 +1761,13 @@ static int serve_launch(cfft_server_s* S, ServeSlot& sl) {
     for (int k = 0; k < 4; k++)
         for (auto& kv : pass[k]) add(std::get<0>(kv.first), 1, kv.second);
     if (host.size() > sl.desc_cap) {
-        if (sl.h_desc) cudaFreeHost(sl.h_desc);
-        if (sl.d_desc) cudaFree(sl.d_desc);
+        if (sl.h_desc) lib_free_host(sl.h_desc);
+        if (sl.d_desc) lib_free(sl.d_desc);
         sl.h_desc = sl.d_desc = nullptr;
         sl.desc_cap = 0;
         const size_t capb = align_up(host.size() * 2, 1 << 16);
-        CUDA_TRY(cudaHostAlloc((void**)&sl.h_desc, capb, cudaHostAllocDefault));
-        CUDA_TRY(cudaMalloc((void**)&sl.d_desc, capb));
+        CUDA_TRY(lib_host_alloc((void**)&sl.h_desc, capb, cudaHostAllocDefault));
+        CUDA_TRY(lib_malloc((void**)&sl.d_desc, capb));
         sl.desc_cap = capb;
     }
     memcpy(sl.h_desc, host.data(), host.size());
@@ -1805,10 +1856,10 @@ static void serve_worker(cfft_server_s* S) {
                 }
                 if (scr + sneed > idle->scratch_cap) {
                     // grow (only when this request alone does not fit; the slot is idle)
-                    if (idle->scratch) cudaFree(idle->scratch);
+                    if (idle->scratch) lib_free(idle->scratch);
                     idle->scratch = nullptr;
                     idle->scratch_cap = 0;
-                    if (cudaMalloc(&idle->scratch, scr + sneed) != cudaSuccess) {
+                    if (lib_malloc(&idle->scratch, scr + sneed) != cudaSuccess) {
                         cudaGetLastError();
                         serve_error(S, "serve: scratch allocation failed");
                         serve_finish(S, std::vector<int64_t>(1, t), -CFFT_ERR_NOMEM);
@@ -1864,16 +1915,16 @@ static void serve_free(cfft_server_s* S) {
         if (sl.st) cudaStreamSynchronize(sl.st);
         if (sl.st) cudaStreamDestroy(sl.st);
         if (sl.ev) cudaEventDestroy(sl.ev);
-        if (sl.h_desc) cudaFreeHost(sl.h_desc);
-        if (sl.d_desc) cudaFree(sl.d_desc);
-        if (sl.scratch) cudaFree(sl.scratch);
+        if (sl.h_desc) lib_free_host(sl.h_desc);
+        if (sl.d_desc) lib_free(sl.d_desc);
+        if (sl.scratch) lib_free(sl.scratch);
     }
     S->slots.clear();
     if (S->dstream) {
         cudaStreamSynchronize(S->dstream);
         cudaStreamDestroy(S->dstream);
     }
-    if (S->dscratch) cudaFree(S->dscratch);
+    if (S->dscratch) lib_free(S->dscratch);
     for (auto& pe : S->dpending) cudaEventDestroy(pe.second);
     for (cudaEvent_t ev : S->evpool) cudaEventDestroy(ev);
     for (auto* m : {&S->plans, &S->dplans})
@@ -1901,7 +1952,7 @@ static int serve_create_impl(cfft_server_s* S, int dtype, int64_t max_inflight_b
             CUDA_TRY(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
             sl.scratch_cap = std::min<size_t>(S->cap / 4, (size_t)1 << 30);
-            CUDA_TRY(cudaMalloc(&sl.scratch, sl.scratch_cap));
+            CUDA_TRY(lib_malloc(&sl.scratch, sl.scratch_cap));
         }
     } else {
         CUDA_TRY(cudaStreamCreateWithFlags(&S->dstream, cudaStreamNonBlocking));
@@ -1919,6 +1970,12 @@ extern "C" {
 int cfft_version(void) { return 100; }
 
 const char* cfft_last_error(void) { return g_err; }
+
+int64_t cfft_debug_alloc_hook(int64_t nth) {
+    g_alloc_seq.store(0);
+    g_alloc_fail_from.store(nth > 0 ? nth : 0);
+    return g_live_allocs.load();
+}
 
 int cfft_plan_create(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags) {
     g_err[0] = 0;
@@ -1966,7 +2023,7 @@ int cfft_plan_create_many(cfft_plan* plan, int64_t n, int64_t batch, int dtype, 
     P->idist = idist;
     P->ostride = ostride;
     P->odist = odist;
-    if (cudaMalloc(&P->strided_work, (size_t)n * batch * elem_bytes(dtype)) != cudaSuccess) {
+    if (lib_malloc(&P->strided_work, (size_t)n * batch * elem_bytes(dtype)) != cudaSuccess) {
         cudaGetLastError();
         plan_free(P);
         delete P;
@@ -2018,8 +2075,8 @@ static int execute_host_staged(cfft_plan_s* P, const void* h_in, void* h_out, in
     cudaStream_t sin = P->host_st[0], scomp = P->host_st[1], sout = P->host_st[2];
     const size_t cap = (size_t)P->host_chunk * tbytes;
     for (int k = 0; k < 3; k++) {
-        if (!P->stage_in[k]) CUDA_TRY(cudaHostAlloc(&P->stage_in[k], cap, cudaHostAllocDefault));
-        if (!P->stage_out[k]) CUDA_TRY(cudaHostAlloc(&P->stage_out[k], cap, cudaHostAllocDefault));
+        if (!P->stage_in[k]) CUDA_TRY(lib_host_alloc(&P->stage_in[k], cap, cudaHostAllocDefault));
+        if (!P->stage_out[k]) CUDA_TRY(lib_host_alloc(&P->stage_out[k], cap, cudaHostAllocDefault));
     }
     const int64_t nch = (P->batch + P->host_chunk - 1) / P->host_chunk;
     auto span = [&](int64_t i, size_t* off, size_t* bytes) {
@@ -2071,7 +2128,7 @@ int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int directi
     if (P->io_half) {
         const size_t bytes = (size_t)P->n * P->batch * 4;
         if (!P->half_dev) {
-            CUDA_TRY(cudaMalloc(&P->half_dev, bytes));
+            CUDA_TRY(lib_malloc(&P->half_dev, bytes));
             P->allocs.push_back(P->half_dev);
         }
         CUDA_TRY(cudaMemcpy(P->half_dev, h_in, bytes, cudaMemcpyHostToDevice));
@@ -2088,12 +2145,20 @@ int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int directi
         c = std::min<int64_t>(c, P->batch);
         if (P->chunk > 0 && P->chunk < P->batch) c = std::max<int64_t>(P->chunk, (c / P->chunk) * P->chunk);
         P->host_chunk = std::min<int64_t>(c, P->batch);
-        for (int i = 0; i < 3; i++) {
-            CUDA_TRY(cudaMalloc(&P->host_buf[i], (size_t)P->host_chunk * tbytes));
-            CUDA_TRY(cudaStreamCreateWithFlags(&P->host_st[i], cudaStreamNonBlocking));
-            CUDA_TRY(cudaEventCreateWithFlags(&P->ev_in[i], cudaEventDisableTiming));
-            CUDA_TRY(cudaEventCreateWithFlags(&P->ev_comp[i], cudaEventDisableTiming));
-            CUDA_TRY(cudaEventCreateWithFlags(&P->ev_out[i], cudaEventDisableTiming));
+        auto setup = [&]() -> int {
+            for (int i = 0; i < 3; i++) {
+                CUDA_TRY(lib_malloc(&P->host_buf[i], (size_t)P->host_chunk * tbytes));
+                CUDA_TRY(cudaStreamCreateWithFlags(&P->host_st[i], cudaStreamNonBlocking));
+                CUDA_TRY(cudaEventCreateWithFlags(&P->ev_in[i], cudaEventDisableTiming));
+                CUDA_TRY(cudaEventCreateWithFlags(&P->ev_comp[i], cudaEventDisableTiming));
+                CUDA_TRY(cudaEventCreateWithFlags(&P->ev_out[i], cudaEventDisableTiming));
+            }
+            return CFFT_OK;
+        };
+        const int rc = setup();
+        if (rc) {
+            host_release(P);        // nothing half-built survives a failed set-up
+            return rc;
         }
         P->host_ready = true;
     }
@@ -2324,11 +2389,11 @@ int cfft_serve_submit(cfft_server server, int64_t n, const void* d_in, void* d_o
         if (need > S->dscratch_cap) {
             if (S->dscratch) {
                 cudaStreamSynchronize(S->dstream);
-                cudaFree(S->dscratch);
+                lib_free(S->dscratch);
             }
             S->dscratch = nullptr;
             S->dscratch_cap = 0;
-            CUDA_TRY(cudaMalloc(&S->dscratch, need));
+            CUDA_TRY(lib_malloc(&S->dscratch, need));
             S->dscratch_cap = need;
         }
         P->scratch[0] = S->dscratch;
@@ -2504,7 +2569,7 @@ int cfft_rfft_plan_create(cfft_rplan* plan, int64_t n, int64_t batch, int dtype,
     const bool even = (n % 2 == 0);
     int rc = plan_create_impl(&R->P, even ? n / 2 : n, batch, dtype, flags);
     if (rc == CFFT_OK && !even) {
-        if (cudaMalloc(&R->scratch, (size_t)n * batch * elem_bytes(dtype)) != cudaSuccess) {
+        if (lib_malloc(&R->scratch, (size_t)n * batch * elem_bytes(dtype)) != cudaSuccess) {
             cudaGetLastError();
             rc = fail(CFFT_ERR_NOMEM, "real-transform scratch allocation failed");
         }
@@ -2574,8 +2639,8 @@ int cfft_rfft_execute_host(cfft_rplan plan, const void* h_in, void* h_out, int d
     const size_t e = elem_bytes(R->dtype);
     const size_t rbytes = (size_t)R->n * R->batch * (e / 2), cbytes = (size_t)(R->n / 2 + 1) * R->batch * e;
     if (!R->d_real) {
-        CUDA_TRY(cudaMalloc(&R->d_real, rbytes + e));
-        CUDA_TRY(cudaMalloc(&R->d_cplx, cbytes));
+        CUDA_TRY(lib_malloc(&R->d_real, rbytes + e));
+        CUDA_TRY(lib_malloc(&R->d_cplx, cbytes));
     }
     int rc;
     if (direction == CFFT_FORWARD) {
@@ -2592,13 +2657,13 @@ int cfft_rfft_execute_host(cfft_rplan plan, const void* h_in, void* h_out, int d
 
 int cfft_rfft_plan_destroy(cfft_rplan plan) {
     if (!plan) return fail(CFFT_ERR_INVALID, "null plan");
-    if (plan->d_real) cudaFree(plan->d_real);
-    if (plan->d_cplx) cudaFree(plan->d_cplx);
+    if (plan->d_real) lib_free(plan->d_real);
+    if (plan->d_cplx) lib_free(plan->d_cplx);
     if (plan->P) {
         plan_free(plan->P);
         delete plan->P;
     }
-    if (plan->scratch) cudaFree(plan->scratch);
+    if (plan->scratch) lib_free(plan->scratch);
     delete plan;
     return CFFT_OK;
 }

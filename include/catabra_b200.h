@@ -209,9 +209,10 @@ int cfft_serve_stats(cfft_server server, int64_t* requests, int64_t* batches, in
 int cfft_serve_destroy(cfft_server server);
 
 /* No counterpart in the reference.  The two-pass FFT for callers that cannot
- * allocate device memory (an allocator-owned or capture-time context): the
- * scratch and twiddle tables live in one fixed __device__ array (32 MiB +
- * 256 KiB per GPU, held until exit), so nothing is allocated.  n must be
+ * allocate device memory (a pool that forbids cudaMalloc, a framework that
+ * owns every allocation): the scratch and twiddle tables live in one fixed
+ * __device__ array (32 MiB + 256 KiB per GPU, held until exit), so nothing is
+ * allocated.  n must be
  * 7-smooth, split as N1*N2 with N1, N2 <= 4096, and hold at most 2^21
  * ComplexF64 / 2^22 ComplexF32 elements; otherwise CFFT_ERR_UNSUPPORTED.
  * The first call on a device does a one-time set-up (make it before any
@@ -219,6 +220,15 @@ int cfft_serve_destroy(cfft_server server);
  * GPU race -- serialise them. */
 int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, const void* d_in, void* d_out,
                              int direction, void* stream);
+
+/* Test hook, no counterpart in the reference (whose failures are Julia
+ * exceptions from @assert / error, src/kernel.jl:113,187, src/prime.jl:6,27,43).
+ * From the nth device or pinned host allocation the library makes after this
+ * call (nth >= 1), every allocation fails as out of memory until the hook is
+ * called again; nth = 0 turns the injection off.  Returns the number of the
+ * library's device and pinned host allocations that are live at the call, so
+ * a test can show that a failed create released what it had allocated. */
+int64_t cfft_debug_alloc_hook(int64_t nth);
 
 /* ABI version (major*100 + minor). */
 int cfft_version(void);

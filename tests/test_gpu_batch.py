@@ -1,9 +1,10 @@
 """GPU tests of the batched form: one graph launch over mixed lengths.
 
 Every transform of a seeded mixed batch (half 7-smooth lengths, half with a
-prime factor up to 65537) must match the single-plan result of the same
-length: 1e-12 relative L2 for ComplexF64, and 1e-5 against the FP64 oracle
-for ComplexF32.
+prime factor up to 65537) is compared with the oracle: 1e-12 relative L2 for
+ComplexF64 (or, where the reference algorithm's own twiddle recurrences
+drift further from the exact DFT, that drift plus 1e-12), and 1e-5 against
+the FP64 oracle for ComplexF32.
 """
 import numpy as np
 import pytest
@@ -16,6 +17,11 @@ pytestmark = pytest.mark.gpu
 
 def rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def bar64(ref, x):
+    """1e-12, or the oracle's own distance to the exact DFT plus 1e-12."""
+    return max(1e-12, rel(ref, np.fft.fft(x)) + 1e-12)
 
 
 @pytest.fixture(scope="module")
@@ -46,8 +52,8 @@ def test_batch_matches_single_plans(cb, dtype, count, hi):
     for i, (o, n) in enumerate(zip(b.offsets, lengths)):
         seg = x[o:o + n]
         if dtype == np.complex128:
-            ref = cb.fft(seg)
-            assert rel(y[o:o + n], ref) < tol, (i, n)
+            ref = oracle.fft(seg)
+            assert rel(y[o:o + n], ref) < bar64(ref, seg), (i, n)
         elif i % 4 == 0:                           # FP32 form vs the FP64 oracle
             ref = oracle.fft(seg.astype(np.complex128))
             assert rel(y[o:o + n], ref) < tol, (i, n)
@@ -68,7 +74,9 @@ def test_batch_two_pass_members(cb, dtype):
     tol = 1e-12 if dtype == np.complex128 else 1e-5
     for o, n in zip(b.offsets, lengths):
         seg = x[o:o + n]
-        ref = cb.fft(seg) if dtype == np.complex128 else oracle.fft(seg.astype(np.complex128))
+        ref = oracle.fft(seg.astype(np.complex128))
+        if dtype == np.complex128:
+            tol = bar64(ref, seg)
         assert rel(y[o:o + n], ref) < tol, n
     b.close()
 

@@ -2,8 +2,9 @@
 
 * Every request's result is bit-for-bit the same whether it runs alone or in
   a mixed micro-batch with other lengths and directions.
-* Results match the single-plan path: 1e-12 relative L2 for ComplexF64,
-  1e-5 against the FP64 oracle for ComplexF32.
+* Results match the oracle: 1e-12 relative L2 for ComplexF64 (plus the
+  reference algorithm's own drift from the exact DFT at large primes), 1e-5
+  against the FP64 oracle for ComplexF32.
 * The direct (per-request) mode matches the oracle too, and a tiny admission
   cap still completes every request.
 """
@@ -81,10 +82,12 @@ def test_serve_matches_plans(cb, dtype):
     tol = 1e-12 if dtype == np.complex128 else 1e-5
     for x, y, d, n in zip(xs, ys, dirs, lengths):
         xx = x.astype(np.complex128)
-        if dtype == np.complex64:
-            ref = (oracle.fft, oracle.ifft, oracle.bfft)[d](xx)
-        else:
-            ref = (cb.fft, cb.ifft, cb.bfft)[d](xx)
+        ref = (oracle.fft, oracle.ifft, oracle.bfft)[d](xx)
+        if dtype == np.complex128:
+            # the reference's twiddle recurrences drift from the exact DFT at
+            # large primes: allow that drift on top of 1e-12
+            exact = (np.fft.fft, np.fft.ifft, lambda v: np.fft.ifft(v) * len(v))[d](xx)
+            tol = max(1e-12, rel(ref, exact) + 1e-12)
         assert rel(y, ref) < tol, (n, d)
 
 
