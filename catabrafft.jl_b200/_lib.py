@@ -57,6 +57,7 @@ SIGNATURES = {
     "cfft_wisdom_forget": (_ci, []),
     "cfft_wisdom_entries": (_i64, []),
     "cfft_debug_alloc_hook": (_i64, [_i64]),
+    "cfft_device_faults": (_ci, [_ci]),
 }
 
 

@@ -30,6 +30,7 @@
 #include <stdint.h>
 
 #include "codelets.cuh"
+#include "tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -298,39 +299,93 @@ __device__ __forceinline__ V r4096_tw(V v, const double2* lo, const double2* hi,
 // input needs no block barrier.  The next transform's input is issued as soon
 // as every thread has read Z (the buffer is free), and lands while stage C
 // computes and stores and while the co-resident CTA works.
-template <typename V>
-__device__ __forceinline__ void r4096_prefetch(const KParams& p, V* buf, int b, int t) {
-    const V* in = (const V*)p.in + (long long)b * p.in_dist;
+//
+// P2A = true: the first pass of a power-of-two length n = N1 x 4096
+// (N1 = 2^p.PA).  Row b is transform b >> PA, i = b & (N1 - 1): the stride-N1
+// subsequence x[i + N1 c], c < 4096 (its 16-byte reads share 32-byte sectors
+// with the neighbouring rows, which the L2 serves from one DRAM fetch).  Its
+// 4096-point DFT is written unscaled as row b of the intermediate
+// (contiguous, at b * out_dist); the column pass applies the four-step
+// twiddle and finishes.
+// Load modes: R4096_PLAIN (cp.async of contiguous transforms), R4096_P2A
+// (cp.async of the stride-N1 subsequences), R4096_P2A_TMA (the same
+// subsequences as 16 tensor copies of 256 elements each, issued by one
+// thread and completing on an mbarrier: the strided gather leaves the
+// load/store queue free; ComplexF64 only, whose 16-byte elements are one
+// aligned box column of the tensor map)
+enum { R4096_PLAIN = 0, R4096_P2A = 1, R4096_P2A_TMA = 2 };
+template <typename V, int MODE>
+__device__ __forceinline__ void r4096_prefetch(const KParams& p, V* buf, int b, int t, const CUtensorMap* tm,
+                                               uint64_t* bar) {
+    if (MODE == R4096_P2A_TMA) {
+        if (t == 0) {
+            const int sh = p.PA;
+            const int tt = b >> sh, i = b & ((1 << sh) - 1);
+            mbar_expect_tx(bar, 4096 * (unsigned)sizeof(V));
 #pragma unroll
-    for (int k = 0; k < 16; k++) cp_async_elem(buf + t + 256 * k, in + t + 256 * k);
+            for (int k = 0; k < 16; k++) tma_load_3d(buf + 256 * k, tm, bar, 2 * i, 256 * k, tt);
+        }
+    } else if (MODE == R4096_P2A) {
+        const int sh = p.PA;
+        const V* in = (const V*)p.in + (long long)(b >> sh) * p.in_dist + (b & ((1 << sh) - 1)) + (t << sh);
+        const long long step = 256LL << sh;
+        // a rolled loop: 16 precomputed strided addresses would stay live
+        // across the last stage and push the FP64 codelets into spills
+#pragma unroll 1
+        for (int k = 0; k < 16; k++, in += step) cp_async_elem(buf + t + 256 * k, in);
+    } else {
+        const V* in = (const V*)p.in + (long long)b * p.in_dist;
+#pragma unroll
+        for (int k = 0; k < 16; k++) cp_async_elem(buf + t + 256 * k, in + t + 256 * k);
+    }
 }
-template <typename V>
-__device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem) {
+template <typename V, int MODE = R4096_PLAIN>
+__device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem, const CUtensorMap* tm = nullptr) {
+    constexpr bool P2A = MODE != R4096_PLAIN;
+    constexpr bool TMA = MODE == R4096_P2A_TMA;
     V* buf = (V*)smem;                          // 16 planes of R4096_PL elements
     double2* tlo = after16(buf + 16 * R4096_PL);
     double2* thi = tlo + 64;
+    uint64_t* bar = (uint64_t*)(thi + 65);
     int b = block_id(p);
     if (b >= p.batch) return;                   // uniform across the CTA
     {
         const int t = opaque_tid();
-        r4096_prefetch(p, buf, b, t);
-        cp_async_commit();
+        if (TMA && t == 0) mbar_init(bar, 1);
         if (t < 64) tlo[t ^ (t >> 3)] = p.t4.lo[t];
         if (t < 65) thi[t] = p.t4.hi[t];
+        if (TMA) __syncthreads();               // the barrier is initialised
+        r4096_prefetch<V, MODE>(p, buf, b, t, tm, bar);
+        if (!TMA) cp_async_commit();
     }
     __syncthreads();                            // tables staged
+    unsigned phase = 0;
     for (; b < p.batch; b += gridDim.x) {
         // re-read per transform: index math hoisted out of the loop would
         // stay live across it and push the FP64 codelets into spills
         const int t = opaque_tid();
         V v[16];
-        cp_async_wait_all();                    // this thread's own input elements
+        bool ok = true;
+        if (TMA) {
+            ok = mbar_wait(bar, phase);         // the row's tensor copies have landed
+            phase ^= 1;
+        } else {
+            cp_async_wait_all();                // this thread's own input elements
+        }
 #pragma unroll
         for (int k = 0; k < 16; k++) v[k] = load_in(p, buf[t + 256 * k]);
         dft<16>(v);
 #pragma unroll
         for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = r4096_tw(v[k1], tlo, thi, (unsigned)(t * k1));
-        __syncthreads();
+        if (TMA) {
+            // every thread leaves together when a copy timed out
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) record_fault(kFaultTmaTimeout);
+                return;
+            }
+        } else {
+            __syncthreads();
+        }
         {
             const int t1 = t & 15, k1 = t >> 4;
 #pragma unroll
@@ -349,12 +404,24 @@ __device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem
         }
         __syncthreads();                        // every Z read: the buffer is free
         const int bn = b + (int)gridDim.x;
-        if (bn < p.batch) r4096_prefetch(p, buf, bn, t);
-        cp_async_commit();
+        if (TMA) {
+            if (t == 0 && bn < p.batch) {
+                fence_proxy_async_smem();       // the reads above precede the copies' writes
+                r4096_prefetch<V, MODE>(p, buf, bn, t, tm, bar);
+            }
+        } else {
+            if (bn < p.batch) r4096_prefetch<V, MODE>(p, buf, bn, t, tm, bar);
+            cp_async_commit();
+        }
         dft<16>(v);
         V* out = (V*)p.out + (long long)b * p.out_dist;
+        if (P2A) {
 #pragma unroll
-        for (int k3 = 0; k3 < 16; k3++) stg_stream(out + t + 256 * k3, store_out(p, v[k3]));
+            for (int k3 = 0; k3 < 16; k3++) out[t + 256 * k3] = v[k3];
+        } else {
+#pragma unroll
+            for (int k3 = 0; k3 < 16; k3++) stg_stream(out + t + 256 * k3, store_out(p, v[k3]));
+        }
     }
 }
 

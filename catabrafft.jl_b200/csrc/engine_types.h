@@ -30,7 +30,7 @@ struct TwoLevel {                 // w_N^e = lo[e & mask] * hi[e >> bits]  (FP64
     int N;
 };
 
-enum { MODE_ROWS = 0, MODE_FOUR = 1, MODE_COLPASS = 2, MODE_ROWPASS = 3 };
+enum { MODE_ROWS = 0, MODE_FOUR = 1, MODE_COLPASS = 2, MODE_ROWPASS = 3, MODE_P2COL = 4, MODE_P2ROW = 5 };
 // kernel selector only (KParams.mode stays MODE_FOUR): the generic four-step
 // kernel instantiated with warp-synchronous sub-transforms
 enum { MODE_FOUR_WARP = 16 };
@@ -66,6 +66,10 @@ struct KParams {
     unsigned char in_user, out_user;  // batched launches: in/out relative to the caller's buffers
     unsigned char pad_[2];
     long long in_off, out_off;    // batched launches: element offsets added to the bases
+    // power-of-two passes: the four-step table of w_n (row pass) and the
+    // single-level table w_N1^e, e < N1 (column pass)
+    TwoLevel t4n;
+    const double2* twN1;
 };
 
 // COLPASS / ROWPASS stage their sub-transform twiddle table in shared memory

@@ -1,7 +1,10 @@
 // kernels.cu -- sm_100a kernel entry points, the registry of statically
 // shaped kernels, and the launcher.
+#include <cudaTypedefs.h>
+
 #include "engine.cuh"
 #include "kernels.h"
+#include "pow2.cuh"
 
 // 256 threads per CTA; FP64 data keeps 2 CTAs/SM resident (128 regs/thread),
 // and so does FP32 data (the exchange staging needs the headroom).
@@ -10,12 +13,12 @@ template <> struct MinBlocks<double2> { static constexpr int value = 2; };
 
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_rows(KParams p) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     rows_body<V, EMAX>(p, smem);
 }
 template <typename V, int EMAX, class K>
 __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_four(KParams p) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     four_body<V, EMAX, K>(p, smem);
 }
 // statically shaped variant with its own residency target: a smaller
@@ -23,7 +26,7 @@ __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) k_four(KPar
 // ComplexF64 CTAs share an SM
 template <typename V, int EMAX, class K, int MB>
 __global__ void __launch_bounds__(CFFT_THREADS, MB) k_four_mb(KParams p) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     four_body<V, EMAX, K>(p, smem);
 }
 // the pass kernels keep three ComplexF32 CTAs resident per SM (80 registers
@@ -33,12 +36,12 @@ template <> struct PassBlocks<double2> { static constexpr int value = 2; };
 
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) k_colpass(KParams p) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     colpass_body<V, EMAX>(p, smem);
 }
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) k_rowpass(KParams p) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     rowpass_body<V, EMAX>(p, smem);
 }
 
@@ -62,26 +65,26 @@ __device__ __forceinline__ const KParams& stage_params(const BatchLaunch& L, KPa
 }
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_rows(BatchLaunch L) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ KParams sp;
     rows_body<V, EMAX>(stage_params<V>(L, &sp), smem);
 }
 template <typename V, int EMAX, class K>
 __global__ void __launch_bounds__(CFFT_THREADS, MinBlocks<V>::value) kb_four(BatchLaunch L) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ KParams sp;
     four_body<V, EMAX, K>(stage_params<V>(L, &sp), smem);
 }
 
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) kb_colpass(BatchLaunch L) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ KParams sp;
     colpass_body<V, EMAX>(stage_params<V>(L, &sp), smem);
 }
 template <typename V, int EMAX>
 __global__ void __launch_bounds__(CFFT_THREADS, PassBlocks<V>::value) kb_rowpass(BatchLaunch L) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ KParams sp;
     rowpass_body<V, EMAX>(stage_params<V>(L, &sp), smem);
 }
@@ -135,14 +138,114 @@ cudaError_t cfft_launch_batch(const void* f, const BatchLaunch& L, unsigned grid
 // than two without spills: more transforms in flight hide the HBM latency.
 template <typename V>
 __global__ void __launch_bounds__(CFFT_THREADS, 3) k_r4096(KParams p) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     r4096_body<V>(p, smem);
 }
 const void* cfft_r4096_kernel(int dtype) {
     return dtype == CFFT_DT_C128 ? (const void*)k_r4096<double2> : (const void*)k_r4096<float2>;
 }
 size_t cfft_r4096_smem(size_t elem_bytes) {
-    return ((16 * R4096_PL * elem_bytes + 15) & ~(size_t)15) + 129 * sizeof(double2);
+    // planes, w_4096 table (129 FP64 entries), one mbarrier (tensor-copy mode)
+    return ((16 * R4096_PL * elem_bytes + 15) & ~(size_t)15) + 129 * sizeof(double2) + 16;
+}
+
+// power-of-two lengths n = N1 x 4096 (pow2.cuh): pass A is the n = 4096
+// kernel over the stride-N1 subsequences (k_p2row), pass B the column DFTs
+// (k_p2col, one kernel per N1); persistent, MB CTAs per SM (ComplexF64 at
+// three has 80 registers and spills, at two none)
+template <typename V, int N1, int MB>
+__global__ void __launch_bounds__(CFFT_THREADS, MB) k_p2col(KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    p2col_body<V, N1>(p, smem);
+}
+template <typename V, int MB>
+__global__ void __launch_bounds__(CFFT_THREADS, MB) k_p2row(KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    r4096_body<V, R4096_P2A>(p, smem);
+}
+// pass A with tensor copies (ComplexF64): tm maps the chunk's input as
+// [transform][c < 4096][2 N1 doubles] (strides N1 x 16 B, in_dist x 16 B)
+template <int MB>
+__global__ void __launch_bounds__(CFFT_THREADS, MB) k_p2row_tma(const __grid_constant__ CUtensorMap tm, KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    r4096_body<double2, R4096_P2A_TMA>(p, smem, &tm);
+}
+template <typename V, int MB> static const void* p2col_for(int N1) {
+    switch (N1) {
+        case 2: return (const void*)k_p2col<V, 2, MB>;
+        case 4: return (const void*)k_p2col<V, 4, MB>;
+        case 8: return (const void*)k_p2col<V, 8, MB>;
+        case 16: return (const void*)k_p2col<V, 16, MB>;
+        case 32: return (const void*)k_p2col<V, 32, MB>;
+        case 64: return (const void*)k_p2col<V, 64, MB>;
+        case 128: return (const void*)k_p2col<V, 128, MB>;
+        case 256: return (const void*)k_p2col<V, 256, MB>;
+        case 512: return (const void*)k_p2col<V, 512, MB>;
+        case 1024: return (const void*)k_p2col<V, 1024, MB>;
+    }
+    return nullptr;
+}
+const void* cfft_p2col_kernel(int dtype, int N1, int mb) {
+    if (dtype == CFFT_DT_C128) return mb == 2 ? p2col_for<double2, 2>(N1) : p2col_for<double2, 3>(N1);
+    return p2col_for<float2, 3>(N1);
+}
+const void* cfft_p2row_tma_kernel(int mb) {
+    return mb == 2 ? (const void*)k_p2row_tma<2> : (const void*)k_p2row_tma<3>;
+}
+// the driver's tensor-map encoder, looked up once through the runtime
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (PFN_cuTensorMapEncodeTiled_v12000)f;
+    }();
+    return fn;
+}
+cudaError_t cfft_launch_p2row_tma(const void* f, const KParams& p, unsigned grid, size_t smem, cudaStream_t st) {
+    auto enc = tensor_map_encoder();
+    if (!f || !enc) return cudaErrorNotSupported;
+    const int N1 = 1 << p.PA;
+    const long long nb = (long long)p.batch >> p.PA;
+    if (nb < 1 || nb > 0x7fffffffLL || ((uintptr_t)p.in & 15)) return cudaErrorInvalidValue;
+    CUtensorMap tm;
+    const cuuint64_t dims[3] = {(cuuint64_t)(2 * N1), 4096, (cuuint64_t)nb};
+    const cuuint64_t strides[2] = {(cuuint64_t)N1 * 16, (cuuint64_t)p.in_dist * 16};
+    const cuuint32_t box[3] = {2, 256, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    // L2 promotion to 256 B: the neighbouring subsequences of the same
+    // lines are read by the CTAs working on the next rows
+    CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)p.in, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(CFFT_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    KParams pc = p;
+    void* args[] = {(void*)&tm, (void*)&pc};
+    cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
+cudaError_t cfft_device_fault_word(unsigned* out, int clear) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_cfft_fault, sizeof(unsigned));
+    if (e == cudaSuccess && clear) {
+        const unsigned z = 0;
+        e = cudaMemcpyToSymbol(g_cfft_fault, &z, sizeof(unsigned));
+    }
+    return e;
+}
+const void* cfft_p2row_kernel(int dtype, int mb) {
+    if (dtype == CFFT_DT_C128) return mb == 2 ? (const void*)k_p2row<double2, 2> : (const void*)k_p2row<double2, 3>;
+    return (const void*)k_p2row<float2, 3>;
+}
+size_t cfft_p2col_smem(size_t elem_bytes, int N1) {
+    return ((4096 * elem_bytes + 15) & ~(size_t)15) + (size_t)N1 * sizeof(double2);
 }
 
 const void* cfft_kernel_for(int mode, int dtype) {

@@ -21,6 +21,22 @@ const void* cfft_static_four(int dtype, int N1, int N2, int C, const unsigned ch
 // plus t4 = the two-level table of w_4096) and its shared memory
 const void* cfft_r4096_kernel(int dtype);
 size_t cfft_r4096_smem(size_t elem_bytes);
+// power-of-two lengths n = N1 x 4096 (N1 = 2 .. 1024, pow2.cuh): pass A
+// (KParams: batch = rows = transforms x N1, PA = log2 N1, t4 = table of
+// w_4096, t4n = table of w_n, staged in shared memory after the kernel's own
+// when pre = 1; shared memory cfft_r4096_smem + the staged table) and pass B
+// (batch = column tiles = transforms x N1, twN1 = w_N1^e for e < N1; shared
+// memory cfft_p2col_smem), built for mb = 3 or 2 CTAs per SM (ComplexF64;
+// ComplexF32 is always 3)
+const void* cfft_p2col_kernel(int dtype, int N1, int mb);
+// pass A with tensor copies (ComplexF64), and its launcher (encodes the
+// tensor map of p.in for this launch)
+const void* cfft_p2row_tma_kernel(int mb);
+cudaError_t cfft_launch_p2row_tma(const void* fn, const KParams& p, unsigned grid, size_t smem, cudaStream_t st);
+// the device fault word (bit 0: a tensor-copy wait timed out), optionally cleared
+cudaError_t cfft_device_fault_word(unsigned* out, int clear);
+const void* cfft_p2row_kernel(int dtype, int mb);
+size_t cfft_p2col_smem(size_t elem_bytes, int N1);
 cudaError_t cfft_prepare_fn(const void* fn, size_t smem, int cluster);
 cudaError_t cfft_launch_fn(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
                            int cluster, cudaStream_t stream);

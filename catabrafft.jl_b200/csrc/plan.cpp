@@ -271,6 +271,7 @@ struct Stage {
     int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
     size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
     unsigned persist = 0;    // kernels that loop over the batch: CTAs to launch at most
+    int launch = 0;          // 1: pass A by tensor copies (its own launcher)
 };
 
 struct Shape {
@@ -282,6 +283,7 @@ struct Shape {
     size_t smem = 0;
     size_t smem_dyn = 0;     // FOUR: the generic (two-buffer) kernels' shared memory
     double score = 0;
+    int var = 0;             // power-of-two passes: 1 = pass A by tensor copies
 };
 
 // Reference-counted device buffer.  Tables that depend only on a length (sub-
@@ -477,6 +479,33 @@ static void conv_kind(int64_t n, int& conv, int64_t& M) {
     M = smooth_ceil(2 * n - 1);
 }
 
+// power-of-two n = N1 x 4096 (N1 = 2 .. 1024) as two register passes
+// (pow2.cuh); V carries the CTAs per SM the kernels are built for
+static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
+    if (n < 8192 || n > (1 << 22) || (n & (n - 1))) return;
+    // V = CTAs per SM of pass A (the n = 4096 kernel over strided rows):
+    // three like the n = 4096 plan, or two (no spills) for ComplexF64;
+    // ComplexF64 pass A by tensor copies (var = 1) first from N1 = 8 (one
+    // 16-byte element per box row pays off once rows are 128 bytes apart;
+    // measured 3-5 % faster there, 2-8 % slower at N1 = 2, 4)
+    const bool tma_first = n >= 8 * 4096;
+    for (int c = 0; c < 4; c++) {
+        const int var = ((c < 2) == tma_first) ? 1 : 0, mb = (c % 2 == 0) ? 3 : 2;
+        if (dtype != CFFT_C128 && (var == 1 || mb == 2)) continue;
+        Shape s;
+        s.var = var;
+        s.mode = MODE_P2COL;
+        s.conv = CONV_NONE;
+        s.M = n;
+        s.N1 = (int)(n / 4096);
+        s.N2 = 4096;
+        s.V = mb;
+        s.ra = radix_split(s.N1);
+        s.rc = {16, 16, 16};
+        out.push_back(s);
+    }
+}
+
 static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) {
     std::vector<Shape> v;
     int conv;
@@ -514,6 +543,10 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
             M2 = smooth_ceil(M2 + 1);
         }
     }
+    // the register passes lead for the lengths they cover
+    std::vector<Shape> p2;
+    pow2_candidates(n, dtype, p2);
+    v.insert(v.begin(), p2.begin(), p2.end());
     return v;
 }
 
@@ -522,6 +555,9 @@ static std::string shape_desc(const Shape& s, int64_t n) {
     std::string pre = c.empty() ? "" : c + "(n=" + std::to_string(n) + ",M=" + std::to_string(s.M) + ")+";
     if (s.mode == MODE_ROWS)
         return pre + "rows(V=" + std::to_string(s.V) + ")[" + join(s.rc) + "]";
+    if (s.mode == MODE_P2COL)
+        return "pow2(N1=" + std::to_string(s.N1) + ",N2=4096,ctas_per_sm=" + std::to_string(s.V) +
+               (s.var == 1 ? ",tma" : "") + ")";
     if (s.mode == MODE_FOUR)
         return pre + "four(C=" + std::to_string(s.C) + ",N1=" + std::to_string(s.N1) +
                ",N2=" + std::to_string(s.N2) + ")[" + join(s.ra) + "|" + join(s.rc) + "]";
@@ -783,6 +819,18 @@ static int make_conv_tables(cfft_plan_s* P, const Shape& sh, KParams& kp, std::s
     }, &kp.spec);
 }
 
+// bytes of intermediate one chunk of a two-pass plan may use: 64 MB for the
+// generic passes (the intermediate then stays in the 126 MB L2) and 512 MB
+// for the power-of-two register passes (measured on B200 at 1 GiB batches:
+// fewer, longer persistent launches beat L2 residency by 7-20 %);
+// CFFT_SCRATCH_MB overrides both (read at plan creation)
+static int64_t scratch_budget(bool pow2 = false) {
+    const char* v = getenv("CFFT_SCRATCH_MB");
+    const long long mb = v ? atoll(v) : 0;
+    if (mb > 0 && mb <= (1LL << 20)) return (int64_t)mb << 20;
+    return (int64_t)(pow2 ? 512 : 64) << 20;
+}
+
 static int plan_build(cfft_plan_s* P, const Shape& sh) {
     P->shape = sh;
     P->stages.clear();
@@ -946,6 +994,81 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         P->chunk = P->batch;
         return CFFT_OK;
     }
+    if (sh.mode == MODE_P2COL) {
+        // power-of-two n = N1 x 4096 (pow2.cuh): pass A = the n = 4096
+        // kernel over the N1 stride-N1 subsequences, into an L2-sized
+        // intermediate; pass B = the N1-point column DFTs into the output
+        const int64_t n = P->n, N1 = sh.N1;
+        const int mb = sh.V;
+        TwoLevel tn, t4096;
+        rc = make_twolevel(P, n, tn);
+        if (rc) return rc;
+        rc = make_twolevel(P, 4096, t4096);
+        if (rc) return rc;
+        const void* w1 = nullptr;
+        rc = cached_table(P, "w1/" + std::to_string(N1), [&](std::vector<unsigned char>& img) {
+            std::vector<double2> v(N1);
+            for (int64_t a = 0; a < N1; a++) v[a] = omega(a, N1, -1);
+            put(img, v);
+        }, &w1);
+        if (rc) return rc;
+        int64_t chunk = std::max<int64_t>(1, scratch_budget(true) / (int64_t)(n * e));
+        chunk = std::min<int64_t>(chunk, P->batch);
+        P->chunk = chunk;
+        P->scratch_bytes = (size_t)chunk * n * e;
+        if (!P->shared_scratch) {
+            CUDA_TRY(lib_malloc(&P->scratch[0], P->scratch_bytes));
+            P->allocs.push_back(P->scratch[0]);
+        }
+        int lg = 0;
+        while ((1LL << lg) < N1) lg++;
+        // pass B: two CTAs per SM for ComplexF64 (no spills), three for
+        // ComplexF32; the w_n table rides in its shared memory when it fits
+        const int mbB = (P->dtype == CFFT_C128) ? 2 : 3;
+        const int nlo = 1 << tn.bits, nhi = (int)((n + nlo - 1) / nlo + 1);
+        const size_t baseB = cfft_p2col_smem(e, (int)N1), tab = (size_t)(nlo + nhi) * sizeof(double2);
+        const bool staged = baseB + tab <= (mbB == 2 ? (size_t)112 * 1024 : (size_t)74 * 1024);
+        Stage a;
+        a.kp = kp;
+        a.kp.mode = MODE_P2ROW;
+        a.kp.N1 = (int)N1;
+        a.kp.N2 = 4096;
+        a.kp.PA = lg;
+        a.kp.t4 = t4096;
+        a.threads = CFFT_THREADS;
+        a.smem = cfft_r4096_smem(e);
+        a.cluster = 1;
+        a.in_sel = 0;
+        a.out_sel = 2;
+        a.fn = sh.var == 1 ? cfft_p2row_tma_kernel(mb) : cfft_p2row_kernel(P->dtype, mb);
+        a.launch = sh.var == 1 ? 1 : 0;
+        Stage b;
+        b.kp = kp;
+        b.kp.mode = MODE_P2COL;
+        b.kp.N1 = (int)N1;
+        b.kp.N2 = 4096;
+        b.kp.twN1 = (const double2*)w1;
+        b.kp.t4n = tn;
+        b.kp.pre = staged ? 1 : 0;
+        b.threads = CFFT_THREADS;
+        b.smem = baseB + (staged ? tab : 0);
+        b.cluster = 1;
+        b.in_sel = 2;
+        b.out_sel = 1;
+        b.fn = cfft_p2col_kernel(P->dtype, (int)N1, mbB);
+        int nsm = 0;
+        CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P->device));
+        for (Stage* st : {&a, &b}) {
+            if (!st->fn) return fail(CFFT_ERR_UNSUPPORTED, "no power-of-two kernel for N1=" + std::to_string(N1));
+            CUDA_TRY(cfft_prepare_fn(st->fn, st->smem, 1));
+            int occ = 0;
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, st->fn, CFFT_THREADS, st->smem));
+            st->persist = (unsigned)(std::max(1, occ) * std::max(1, nsm));
+        }
+        P->stages.push_back(a);
+        P->stages.push_back(b);
+        return CFFT_OK;
+    }
     // two HBM passes per FFT_M (and two FFT_M for a convolution)
     const int64_t N1 = sh.N1, N2 = sh.N2, M = sh.M;
     const int64_t PC = N2 + ((N2 % 2 == 0) ? 1 : 0);
@@ -967,7 +1090,7 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
     if (rc) return rc;
     // chunk the batch so the scratch of one chunk stays within ~64 MB (L2 sized)
     const int nscr = (sh.conv == CONV_NONE) ? 1 : 2;
-    int64_t chunk = std::max<int64_t>(1, (int64_t)(64LL << 20) / (int64_t)(M * e * nscr));
+    int64_t chunk = std::max<int64_t>(1, scratch_budget() / (int64_t)(M * e * nscr));
     chunk = std::min<int64_t>(chunk, P->batch);
     P->chunk = chunk;
     P->scratch_bytes = (size_t)chunk * M * e;
@@ -1077,6 +1200,8 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             kp.dir = dir;
             kp.scale = (dir == CFFT_INVERSE) ? 1.0 / (double)n : 1.0;
             kp.batch = (int)nb;
+            const bool p2 = kp.mode == MODE_P2COL || kp.mode == MODE_P2ROW;
+            if (p2) kp.batch = (int)(nb * kp.N1);     // column tiles / rows
             const char* user_in = (const char*)in + (size_t)b0 * idist * e;
             char* user_out = (char*)out + (size_t)b0 * odist * e;
             auto sel = [&](int w) -> void* {
@@ -1087,13 +1212,16 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             auto dist = [&](int sel) -> int64_t { return sel >= 2 ? P->shape.M : sel == 0 ? idist : odist; };
             kp.in_dist = dist(s.in_sel);
             kp.out_dist = dist(s.out_sel);
+            if (kp.mode == MODE_P2ROW) kp.out_dist = 4096;  // rows of the intermediate
             unsigned grid;
-            if (kp.mode == MODE_ROWS) grid = (unsigned)((nb + kp.V - 1) / kp.V);
+            if (p2) grid = (unsigned)kp.batch;
+            else if (kp.mode == MODE_ROWS) grid = (unsigned)((nb + kp.V - 1) / kp.V);
             else if (kp.mode == MODE_FOUR) grid = (unsigned)(nb * kp.C);
             else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
             else grid = (unsigned)(nb * (kp.N1 / kp.V));
             if (s.persist && grid > s.persist) grid = s.persist;
-            cudaError_t ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
+            cudaError_t ce = s.launch == 1 ? cfft_launch_p2row_tma(s.fn, kp, grid, s.smem, st)
+                                           : cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             if (ce != cudaSuccess)
                 return fail(CFFT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
         }
@@ -1143,6 +1271,7 @@ static std::string shape_signature(const Shape& s) {
     for (int x : s.ra) r += " " + std::to_string(x);
     r += " c";
     for (int x : s.rc) r += " " + std::to_string(x);
+    if (s.var) r += " v" + std::to_string(s.var);
     return r;
 }
 static bool wisdom_lookup(const WisdomKey& k, std::string& sig) {
@@ -1342,6 +1471,7 @@ static int build_shared_plan(int64_t n, int dtype, int flags, int device, cfft_p
     P->shared_scratch = true;
     int rc = fail(CFFT_ERR_UNSUPPORTED, "no execution shape for n=" + std::to_string(n));
     for (auto& c : cands) {
+        if (c.mode == MODE_P2COL) continue;    // not descriptor driven: batched and served forms skip it
         rc = plan_build(P, c);
         if (rc == CFFT_OK) break;
         plan_free(P);
@@ -1970,6 +2100,17 @@ extern "C" {
 int cfft_version(void) { return 100; }
 
 const char* cfft_last_error(void) { return g_err; }
+
+int cfft_device_faults(int clear) {
+    unsigned w = 0;
+    cudaError_t e = cfft_device_fault_word(&w, clear);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(CFFT_ERR_CUDA, std::string("device fault word: ") + cudaGetErrorString(e));
+        return -1;
+    }
+    return (int)w;
+}
 
 int64_t cfft_debug_alloc_hook(int64_t nth) {
     g_alloc_seq.store(0);

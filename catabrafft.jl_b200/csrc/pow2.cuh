@@ -1,0 +1,266 @@
+// pow2.cuh -- power-of-two lengths n = N1 x 4096 (N1 = 2 .. 1024) as two
+// register passes.
+//
+// With x[i + N1 c] (i < N1, c < 4096) and X[q + 4096 r] (q < 4096, r < N1):
+//   X[q + 4096 r] = sum_i w_N1^(i r) [ w_n^(i q) sum_c x[i + N1 c] w_4096^(c q) ]
+// Pass A (r4096_body<V, true>): for every i, the 4096-point DFT of the
+//   stride-N1 subsequence, written as row i of an intermediate Z (N1 x 4096
+//   per transform, sized to stay in L2).
+// Pass B (this file): for every column q of Z, the four-step twiddle
+//   w_n^(i q) and the N1-point DFT over i, written to X[q + 4096 r] -- row r
+//   of the output viewed as N1 x 4096, so a tile of adjacent columns stores
+//   contiguous segments.  A thread's twiddles for one column q and rows
+//   i0 + d m are w_n^(q i0) (w_n^(q d))^m: two lookups of the FP64 two-level
+//   table and an FP64 recurrence of at most 15 products (relative error a
+//   few 1e-15), rounded once to the data type.
+// The strided accesses are reads (pass A), which the L2 merges; every store
+// to HBM is a contiguous segment.  The reference's pass structure for these
+// lengths is the layered radix-8 Stockham sequence
+// (src/radix_2_codelets.jl:279-447); here each pass keeps 16 elements per
+// thread in registers.
+//
+// A column tile of pass B is VC = 4096 / N1 adjacent columns (4096 elements,
+// 16 per thread, 256 threads).  Element k of thread tid is staged by cp.async
+// in shared-memory slot tid + 256 k, which is tile position (row, col) =
+// (slot / VC, slot % VC): each thread's copies land where it reads them, so
+// the input needs no block barrier, and the next tile can stream in as soon
+// as the buffer is free (persistent CTAs).  Once a tile is in shared memory
+// its intermediate lines are dropped from L2 without a write-back.
+//
+// The column DFT of length N1 = 16^A * RL (RL in {1, 2, 4, 8}) runs as
+// decimation-in-frequency Stockham stages: stage s of radix r splits every
+// current sub-transform of length Ls = N1 / 16^s as t = t' + (Ls / r) m,
+// does DFT_r over m, multiplies by w_Ls^(t' k) and leaves sub-transform
+// K + 16^s k of length Ls / r.  Between stages, element (K, t) of column j
+// sits at ((K Ls + t) VC + j): lanes run over adjacent columns, so every
+// shared access of a quarter-warp is 8 consecutive 16-byte slots when VC >= 8
+// (ComplexF64) and 16 consecutive 8-byte slots when VC >= 16 (ComplexF32).
+// The output index of a column is K + 16^(S-1) k of the last stage.
+#pragma once
+#include "engine.cuh"
+
+__host__ __device__ constexpr int p2_log16(int n) { return (n >= 16 && n % 16 == 0) ? 1 + p2_log16(n / 16) : 0; }
+__host__ __device__ constexpr int p2_pow16(int a) { return a == 0 ? 1 : 16 * p2_pow16(a - 1); }
+__host__ __device__ constexpr int p2_log2(int n) { return n <= 1 ? 0 : 1 + p2_log2(n / 2); }
+
+template <int N1_> struct P2Col {
+    static constexpr int N1 = N1_;
+    static constexpr int LGN1 = p2_log2(N1);
+    static constexpr int VC = 4096 / N1;                  // columns per tile
+    static constexpr int LGVC = p2_log2(VC);
+    static constexpr int A = p2_log16(N1);                // radix-16 stages
+    static constexpr int RL = N1 / p2_pow16(A);           // last radix, 1 = none
+    static constexpr int S = A + (RL > 1 ? 1 : 0);        // stages
+    static constexpr int TPC = N1 >= 16 ? N1 / 16 : 1;    // threads per column
+    static constexpr int CPT = N1 >= 16 ? 1 : 16 / N1;    // columns per thread (N1 < 16)
+    static constexpr bool kExchange = S > 1;              // stages talk through shared memory
+    static_assert(N1 >= 2 && N1 <= 1024 && (N1 & (N1 - 1)) == 0, "N1 is a power of two in [2, 1024]");
+    static_assert(N1 >= 16 || A == 0, "");
+};
+
+// w_n^e from the FP64 two-level table
+__device__ __forceinline__ double2 p2_wn(const double2* lo, const double2* hi, int bits, unsigned e) {
+    return cmul(lo[e & ((1u << bits) - 1)], hi[e >> bits]);
+}
+// x w_N1^e from the single-level FP64 table (exactly rounded, once to V)
+template <typename V>
+__device__ __forceinline__ V p2_tw_stage(V v, const double2* tw, unsigned e) {
+    return e ? cmul(v, fromd<V>(tw[e])) : v;
+}
+// L2 lines of the intermediate that no one reads again are dropped without a
+// write-back to HBM (their contents become undefined)
+__device__ __forceinline__ void l2_discard_line(const void* p) {
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+template <typename V, class PC>
+__device__ __forceinline__ void p2col_prefetch(const KParams& p, V* buf, int tile, int tid) {
+    // tile -> transform tile / N1, first column (tile % N1) VC
+    const int tt = tile >> PC::LGN1;
+    const int c0 = (tile & (PC::N1 - 1)) * PC::VC;
+    const V* in = (const V*)p.in + (long long)tt * p.in_dist + c0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int slot = tid + 256 * k;
+        cp_async_elem(buf + slot, in + ((slot >> PC::LGVC) << 12) + (slot & (PC::VC - 1)));
+    }
+}
+
+// discard the tile's intermediate lines once every thread's copies of them
+// have landed (caller synchronised): thread tid owns slots tid + 256 k; when
+// a tile row spans whole 128-byte lines, the first thread of each line drops it
+template <typename V, class PC>
+__device__ __forceinline__ void p2col_discard(const KParams& p, int tile, int tid) {
+    constexpr int EPL = 128 / (int)sizeof(V);
+    if constexpr (PC::VC >= EPL) {
+        if ((tid & (EPL - 1)) == 0) {
+            const int tt = tile >> PC::LGN1;
+            const int c0 = (tile & (PC::N1 - 1)) * PC::VC;
+            const V* in = (const V*)p.in + (long long)tt * p.in_dist + c0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int slot = tid + 256 * k;
+                l2_discard_line(in + ((slot >> PC::LGVC) << 12) + (slot & (PC::VC - 1)));
+            }
+        }
+    }
+}
+// an output of the last stage: X[q + 4096 r] = row r, column q
+template <typename V>
+__device__ __forceinline__ void p2col_store(const KParams& p, V* out, int col, int r, V v) {
+    stg_stream(out + ((long long)r << 12) + col, store_out(p, v));
+}
+
+// radix-r DFT of v[g r .. g r + r)
+template <int R, typename V> __device__ __forceinline__ void p2_dft_group(V* v) {
+    dft<R>(*reinterpret_cast<V(*)[R]>(v));
+}
+
+// stage s >= 1 of a column of N1 >= 32 (an exchange through shared memory)
+template <typename V, class PC, int s>
+__device__ __forceinline__ void p2col_stage(const KParams& p, V* buf, const double2* tw, int tile) {
+    constexpr int r = (s < PC::A) ? 16 : PC::RL;
+    constexpr int Ls = PC::N1 / p2_pow16(s);
+    constexpr int nb = Ls / r;
+    constexpr int G = 16 / r;
+    constexpr int KR = p2_pow16(s);
+    constexpr bool last = (s == PC::S - 1);
+    const int tid = opaque_tid();
+    const int j = tid & (PC::VC - 1), b = tid >> PC::LGVC;
+    V v[16];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        const int beta = b + PC::TPC * g;
+        const int tp = beta & (nb - 1), K = beta / nb;
+#pragma unroll
+        for (int m = 0; m < r; m++) v[g * r + m] = buf[((K * Ls + tp + nb * m) << PC::LGVC) + j];
+    }
+    __syncthreads();                            // every read of this stage before the writes
+    if (last) {
+        // the buffer is free: the next tile streams in while this one finishes
+        const int tn = tile + (int)gridDim.x;
+        if (tn < p.batch) p2col_prefetch<V, PC>(p, buf, tn, tid);
+        cp_async_commit();
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++) p2_dft_group<r>(v + g * r);
+    if (last) {
+        const int tt = tile >> PC::LGN1;
+        const int c = (tile & (PC::N1 - 1)) * PC::VC + j;
+        V* out = (V*)p.out + (long long)tt * p.out_dist;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int K = b + PC::TPC * g;      // nb == 1
+#pragma unroll
+            for (int k = 0; k < r; k++) p2col_store(p, out, c, K + KR * k, v[g * r + k]);
+        }
+    } else {
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int beta = b + PC::TPC * g;
+            const int tp = beta & (nb - 1), K = beta / nb;
+#pragma unroll
+            for (int k = 0; k < r; k++) {
+                const V w = p2_tw_stage(v[g * r + k], tw, (unsigned)(tp * k * (PC::N1 / Ls)));
+                buf[(((K + KR * k) * nb + tp) << PC::LGVC) + j] = w;
+            }
+        }
+        __syncthreads();
+    }
+}
+template <typename V, class PC, int s>
+__device__ __forceinline__ void p2col_stages(const KParams& p, V* buf, const double2* tw, int tile) {
+    if constexpr (s < PC::S) {
+        p2col_stage<V, PC, s>(p, buf, tw, tile);
+        p2col_stages<V, PC, s + 1>(p, buf, tw, tile);
+    }
+}
+
+// Pass B body: p.in = the intermediate (N1 x 4096 per transform, at
+// in_dist), p.out = the output (at out_dist), p.batch = tiles (transforms x
+// N1), p.twN1 = w_N1^e for e < N1 (staged in shared memory after the tile),
+// p.t4n = the two-level table of w_n (staged after it when p.pre != 0).
+// Pass A conjugated the input of the inverse directions; the stores here
+// conjugate and scale.
+template <typename V, int N1>
+__device__ __forceinline__ void p2col_body(const KParams& p, unsigned char* smem) {
+    using PC = P2Col<N1>;
+    V* buf = (V*)smem;                          // 4096 elements
+    double2* tw = after16(buf + 4096);          // N1 entries
+    int tile = block_id(p);
+    if (tile >= p.batch) return;                // uniform across the CTA
+    const int bits = p.t4n.bits;
+    const double2 *lo = p.t4n.lo, *hi = p.t4n.hi;
+    {
+        const int tid = opaque_tid();
+        p2col_prefetch<V, PC>(p, buf, tile, tid);
+        cp_async_commit();
+        for (int i = tid; i < N1; i += 256) tw[i] = p.twN1[i];
+        if (p.pre) {
+            double2* ts = tw + N1;
+            const int nlo = 1 << bits, nhi = (p.t4n.N + nlo - 1) / nlo + 1;
+            for (int i = tid; i < nlo + nhi; i += 256) ts[i] = (i < nlo) ? p.t4n.lo[i] : p.t4n.hi[i - nlo];
+            lo = ts;
+            hi = ts + nlo;
+        }
+        __syncthreads();
+    }
+    for (; tile < p.batch; tile += gridDim.x) {
+        const int tid = opaque_tid();
+        V v[16];
+        cp_async_wait_all();                    // this thread's own slots
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] = buf[tid + 256 * k];
+        const int tt = tile >> PC::LGN1;
+        const int c0 = (tile & (N1 - 1)) * PC::VC;
+        V* out = (V*)p.out + (long long)tt * p.out_dist;
+        if constexpr (N1 <= 16) {
+            // no exchange: once the warp's copies have landed (a discarded
+            // line spans lanes of one warp) the next tile is issued into
+            // these slots right away
+            __syncwarp();
+            p2col_discard<V, PC>(p, tile, tid);
+            const int tn = tile + (int)gridDim.x;
+            if (tn < p.batch) p2col_prefetch<V, PC>(p, buf, tn, tid);
+            cp_async_commit();
+#pragma unroll
+            for (int g = 0; g < PC::CPT; g++) {
+                // column q, rows m < N1: twiddles (w_n^q)^m
+                V u[N1];
+                const unsigned q = (unsigned)(c0 + tid + 256 * g);
+                const double2 st = p2_wn(lo, hi, bits, q);
+                double2 w = st;
+                u[0] = v[g];
+#pragma unroll
+                for (int m = 1; m < N1; m++) {
+                    u[m] = cmul(v[g + PC::CPT * m], fromd<V>(w));
+                    if (m + 1 < N1) w = cmul(w, st);
+                }
+                dft<N1>(u);
+#pragma unroll
+                for (int k = 0; k < N1; k++) p2col_store(p, out, (int)q, k, u[k]);
+            }
+        } else {
+            const int j = tid & (PC::VC - 1), b = tid >> PC::LGVC;
+            {
+                // column q = c0 + j, rows b + TPC k: w_n^(q b) (w_n^(q TPC))^k
+                const unsigned q = (unsigned)(c0 + j);
+                double2 w = p2_wn(lo, hi, bits, q * (unsigned)b);
+                const double2 st = p2_wn(lo, hi, bits, q * (unsigned)PC::TPC);
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    v[k] = cmul(v[k], fromd<V>(w));
+                    if (k < 15) w = cmul(w, st);
+                }
+            }
+            dft<16>(v);
+            // stage 0: twiddle w_N1^(b k), back into this thread's own
+            // slots (row b + TPC k of the tile = sub-transform k, t = b)
+#pragma unroll
+            for (int k = 0; k < 16; k++) buf[tid + 256 * k] = p2_tw_stage(v[k], tw, (unsigned)(b * k));
+            __syncthreads();                    // every copy of the tile has landed and been read
+            p2col_discard<V, PC>(p, tile, tid);
+            p2col_stages<V, PC, 1>(p, buf, tw, tile);
+        }
+    }
+}

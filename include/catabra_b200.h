@@ -221,6 +221,13 @@ int cfft_serve_destroy(cfft_server server);
 int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, const void* d_in, void* d_out,
                              int direction, void* stream);
 
+/* No counterpart in the reference.  The device fault word of the current
+ * device: bit 0 is set when a kernel's bounded wait on its tensor copies (an
+ * mbarrier) gave up, in which case that launch left its results incomplete.
+ * Returns the word (0 = no fault; cleared when `clear` is nonzero), or -1 if
+ * it could not be read (cfft_last_error() has the reason). */
+int cfft_device_faults(int clear);
+
 /* Test hook, no counterpart in the reference (whose failures are Julia
  * exceptions from @assert / error, src/kernel.jl:113,187, src/prime.jl:6,27,43).
  * From the nth device or pinned host allocation the library makes after this

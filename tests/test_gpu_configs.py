@@ -103,13 +103,14 @@ def test_bench_configuration_rows_vs_oracle(cb, n):
         assert rel(zs[i], oracle.ifft(xs[i])) < TOL64, (n, r, "ifft")
 
 
-@pytest.mark.parametrize("n,batch,dtype", [(1 << 16, 300, np.complex64), (1 << 20, 9, np.complex128),
+@pytest.mark.parametrize("n,batch,dtype", [(3 ** 10, 300, np.complex64), (3 ** 12, 9, np.complex128),
                                            (999983, 3, np.complex128)])
 def test_two_pass_across_scratch_chunks(cb, n, batch, dtype):
-    """Two-pass plans whose batch is processed in several scratch chunks (the
-    intermediate of one chunk is sized to stay in L2): ComplexF32 2^16 x 300,
-    ComplexF64 2^20 x 9, and the prime 999983, whose convolution exceeds a
-    cluster and runs as a two-pass Bluestein plan, one transform per chunk."""
+    """Generic two-pass plans whose batch is processed in several scratch
+    chunks (the intermediate of one chunk is sized to stay in L2):
+    ComplexF32 3^10 x 300, ComplexF64 3^12 x 9, and the prime 999983, whose
+    convolution exceeds a cluster and runs as a two-pass Bluestein plan, one
+    transform per chunk.  (Power-of-two chunking is covered below.)"""
     import torch
     code = cb.C128 if dtype == np.complex128 else cb.C64
     x = _device_batch(torch, n, batch, dtype, seed=n + batch)
@@ -161,3 +162,80 @@ def test_register_kernel_persistent_loop(cb, dtype, tol):
             errs = np.linalg.norm(o - r, axis=1) / np.linalg.norm(r, axis=1)
             assert errs.max() < tol, (batch, d, int(errs.argmax()), float(errs.max()))
         assert np.array_equal(t.cpu().numpy(), outs[0].cpu().numpy())
+
+
+def _greedy_split(L):
+    out = []
+    while L > 1:
+        r = next(r for r in (16, 9, 8, 7, 5, 4, 3, 2) if L % r == 0)
+        out.append(r)
+        L //= r
+    return out
+
+
+def _pow2_check(cb, n, batch, dtype, desc_part, flags=0):
+    import torch
+    code = cb.C128 if dtype == np.complex128 else cb.C64
+    tol = TOL64 if dtype == np.complex128 else TOL32
+    x = _device_batch(torch, n, batch, dtype, seed=n + batch)
+    with _CPlan(cb, n, batch, code, flags) as p:
+        assert desc_part in p.describe(), (n, p.describe())
+        outs = [_execute(cb, p.h, x, d) for d in (cb.FORWARD, cb.INVERSE, cb.BACKWARD)]
+        t = x.clone()
+        _execute(cb, p.h, t, cb.FORWARD, out=t)                   # in place
+        torch.cuda.synchronize()
+    rows = sorted({0, batch // 2, batch - 1})
+    xs = x[rows].cpu().numpy().astype(np.complex128)
+    for d, o in zip((oracle.FWD, oracle.INV, oracle.BWD), outs):
+        ref = oracle.transform(xs, d)
+        got = o[rows].cpu().numpy()
+        errs = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert errs.max() < tol, (n, batch, d, float(errs.max()))
+    assert np.array_equal(t[rows].cpu().numpy(), outs[0][rows].cpu().numpy())
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_pow2_register_passes(cb, dtype):
+    """Power-of-two n = N1 x 4096 (N1 = 2 .. 1024): pass A (the n = 4096
+    kernel over the stride-N1 subsequences; ComplexF64 loads them by tensor
+    copies) and pass B (the N1-point column DFTs).  Batches give every
+    persistent CTA several rows and tiles (prefetch into the freed buffer),
+    and the largest lengths run several intermediate chunks.  Forward,
+    inverse, backward and in place against the oracle; no kernel recorded a
+    timed-out wait."""
+    cb._lib.LIB.cfft_device_faults(1)
+    for e in range(13, 23):
+        n = 1 << e
+        N1 = n // 4096
+        batch = max(3, 2048 // N1 + 1)
+        tag = ",tma)" if dtype == np.complex128 and N1 >= 8 else ")"
+        _pow2_check(cb, n, batch, dtype, f"pow2(N1={N1},N2=4096,ctas_per_sm=3{tag}")
+    assert cb._lib.LIB.cfft_device_faults(1) == 0
+
+
+def test_pow2_other_variants(cb, tmp_path):
+    """Every ComplexF64 build of pass A, reached through wisdom entries for
+    MEASURE plans: cp.async loads and tensor copies, at three and at two CTAs
+    per SM."""
+    variants = [(3, 0, ")"), (2, 0, ")"), (3, 1, ",tma)"), (2, 1, ",tma)")]
+    cases = [(1 << 13, 300), (1 << 16, 40), (1 << 20, 3), (1 << 22, 9)]
+    cb._lib.LIB.cfft_device_faults(1)
+    for mb, var, tag in variants:
+        lines = ["catabra-b200-wisdom 1"]
+        for n, batch in cases:
+            N1 = n // 4096
+            sig = f"4 0 {n} {N1} 4096 1 {mb} a {' '.join(map(str, _greedy_split(N1)))} c 16 16 16"
+            if var:
+                sig += f" v{var}"
+            lines.append(f"{n} {batch} 0 {cb.MEASURE} | {sig}")
+        path = tmp_path / f"w{mb}{var}.txt"
+        path.write_text("\n".join(lines) + "\n")
+        cb.forget_wisdom()
+        cb.import_wisdom(str(path))
+        try:
+            for n, batch in cases:
+                _pow2_check(cb, n, batch, np.complex128, f"pow2(N1={n // 4096},N2=4096,ctas_per_sm={mb}{tag}",
+                            flags=cb.MEASURE)
+        finally:
+            cb.forget_wisdom()
+    assert cb._lib.LIB.cfft_device_faults(1) == 0
