@@ -2,6 +2,7 @@
 // shaped kernels, and the launcher.
 #include <cudaTypedefs.h>
 
+#include "convc.cuh"
 #include "engine.cuh"
 #include "kernels.h"
 #include "pow2.cuh"
@@ -246,6 +247,33 @@ const void* cfft_p2row_kernel(int dtype, int mb) {
 }
 size_t cfft_p2col_smem(size_t elem_bytes, int N1) {
     return ((4096 * elem_bytes + 15) & ~(size_t)15) + (size_t)N1 * sizeof(double2);
+}
+
+// Rader on a cluster of C register-FFT CTAs (convc.cuh), MB CTAs per SM
+// (ComplexF64 at three: 80 registers and some spills; at two: none)
+template <typename V, int C, int MB>
+__global__ void __launch_bounds__(CFFT_THREADS, MB) k_convc(KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    convc_rader_body<V, C>(p, smem);
+}
+template <typename V, int MB> static const void* convc_for(int C) {
+    switch (C) {
+        case 3: return (const void*)k_convc<V, 3, MB>;
+        case 4: return (const void*)k_convc<V, 4, MB>;
+        case 5: return (const void*)k_convc<V, 5, MB>;
+        case 7: return (const void*)k_convc<V, 7, MB>;
+        case 8: return (const void*)k_convc<V, 8, MB>;
+    }
+    return nullptr;
+}
+const void* cfft_convc_kernel(int dtype, int C, int mb) {
+    if (dtype == CFFT_DT_C128) return mb == 2 ? convc_for<double2, 2>(C) : convc_for<double2, 3>(C);
+    return convc_for<float2, 3>(C);
+}
+size_t cfft_convc_smem(size_t elem_bytes) {
+    // planes, w_4096 table (129), partial sum (1), reduction scratch (32) and
+    // the total for y[0] (1), FP64
+    return ((16 * R4096_PL * elem_bytes + 15) & ~(size_t)15) + (129 + 1 + 33) * sizeof(double2);
 }
 
 const void* cfft_kernel_for(int mode, int dtype) {

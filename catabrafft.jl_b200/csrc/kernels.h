@@ -33,6 +33,11 @@ const void* cfft_p2col_kernel(int dtype, int N1, int mb);
 // tensor map of p.in for this launch)
 const void* cfft_p2row_tma_kernel(int mb);
 cudaError_t cfft_launch_p2row_tma(const void* fn, const KParams& p, unsigned grid, size_t smem, cudaStream_t st);
+// Rader for primes on a cluster of C in {3, 4, 5, 7, 8} register 4096-point
+// CTAs (convc.cuh; M = 4096 C), built for mb = 3 or 2 CTAs per SM
+// (ComplexF64; ComplexF32 is always 3), and its shared memory
+const void* cfft_convc_kernel(int dtype, int C, int mb);
+size_t cfft_convc_smem(size_t elem_bytes);
 // the device fault word (bit 0: a tensor-copy wait timed out), optionally cleared
 cudaError_t cfft_device_fault_word(unsigned* out, int clear);
 const void* cfft_p2row_kernel(int dtype, int mb);
