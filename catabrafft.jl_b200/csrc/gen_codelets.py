@@ -27,7 +27,7 @@ from decimal import Decimal, getcontext
 from fractions import Fraction
 
 getcontext().prec = 60
-RADICES = [2, 3, 4, 5, 7, 8, 9, 16]
+RADICES = [2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 14, 15, 16, 18]
 
 
 def _pi() -> Decimal:

@@ -4,6 +4,7 @@
 
 #include "convc.cuh"
 #include "engine.cuh"
+#include "mixc.cuh"
 #include "kernels.h"
 #include "pow2.cuh"
 
@@ -274,6 +275,34 @@ size_t cfft_convc_smem(size_t elem_bytes) {
     // planes, w_4096 table (129), partial sum (1), reduction scratch (32) and
     // the total for y[0] (1), FP64
     return ((16 * R4096_PL * elem_bytes + 15) & ~(size_t)15) + (129 + 1 + 33) * sizeof(double2);
+}
+
+// mixed-radix lengths n = C L on a cluster of C register L-point CTAs
+// (mixc.cuh), two CTAs per SM
+template <typename V, class S>
+__global__ void __launch_bounds__(S::T, 2) k_mixc(KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    mixc_body<V, S>(p, smem);
+}
+struct MixEntry {
+    int n, C, L, threads;
+    const void* fn[2];            // ComplexF64, ComplexF32
+};
+// 30240 = 7 x 4320, 4320 = 16 x 18 x 15 (the mixed-radix benchmark length)
+using Mix30240 = MixShape<7, 16, 18, 15, 288>;
+static const MixEntry kMix[] = {
+    {30240, 7, 4320, 288, {(const void*)k_mixc<double2, Mix30240>, (const void*)k_mixc<float2, Mix30240>}},
+};
+int cfft_mixc_lookup(long long n, int dtype, const void** fn, int* C, int* L, int* threads) {
+    for (const auto& m : kMix) {
+        if (m.n != n) continue;
+        *fn = m.fn[dtype == CFFT_DT_C128 ? 0 : 1];
+        *C = m.C;
+        *L = m.L;
+        *threads = m.threads;
+        return 1;
+    }
+    return 0;
 }
 
 const void* cfft_kernel_for(int mode, int dtype) {

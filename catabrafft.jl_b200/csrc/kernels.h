@@ -38,6 +38,9 @@ cudaError_t cfft_launch_p2row_tma(const void* fn, const KParams& p, unsigned gri
 // (ComplexF64; ComplexF32 is always 3), and its shared memory
 const void* cfft_convc_kernel(int dtype, int C, int mb);
 size_t cfft_convc_smem(size_t elem_bytes);
+// mixed-radix lengths with a cluster kernel of C register L-point CTAs
+// (mixc.cuh): 1 and the kernel, C, L and threads per CTA, else 0
+int cfft_mixc_lookup(long long n, int dtype, const void** fn, int* C, int* L, int* threads);
 // the device fault word (bit 0: a tensor-copy wait timed out), optionally cleared
 cudaError_t cfft_device_fault_word(unsigned* out, int clear);
 const void* cfft_p2row_kernel(int dtype, int mb);

@@ -531,6 +531,23 @@ static void convc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     }
 }
 
+// mixed-radix lengths with a cluster kernel of register L-point CTAs
+// (mixc.cuh): n = C x L
+static void mixc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
+    const void* fn = nullptr;
+    int C = 0, L = 0, T = 0;
+    if (!cfft_mixc_lookup(n, dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, &fn, &C, &L, &T)) return;
+    Shape s;
+    s.mode = MODE_MIXC;
+    s.conv = CONV_NONE;
+    s.M = n;
+    s.N1 = C;
+    s.N2 = L;
+    s.C = C;
+    s.V = T;
+    out.push_back(s);
+}
+
 static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) {
     std::vector<Shape> v;
     int conv;
@@ -572,6 +589,7 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
     std::vector<Shape> reg;
     pow2_candidates(n, dtype, reg);
     convc_candidates(n, dtype, reg);
+    mixc_candidates(n, dtype, reg);
     v.insert(v.begin(), reg.begin(), reg.end());
     return v;
 }
@@ -581,6 +599,9 @@ static std::string shape_desc(const Shape& s, int64_t n) {
     std::string pre = c.empty() ? "" : c + "(n=" + std::to_string(n) + ",M=" + std::to_string(s.M) + ")+";
     if (s.mode == MODE_ROWS)
         return pre + "rows(V=" + std::to_string(s.V) + ")[" + join(s.rc) + "]";
+    if (s.mode == MODE_MIXC)
+        return "cluster(C=" + std::to_string(s.C) + ",L=" + std::to_string(s.N2) + " per CTA,threads=" +
+               std::to_string(s.V) + ")";
     if (s.mode == MODE_CONVC)
         return pre + "cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_P2COL)
@@ -922,6 +943,43 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
             if (rc) return rc;
             kp.spec = (const double2*)d;
         }
+    }
+    if (sh.mode == MODE_MIXC) {
+        // n = C x L on a cluster of C register L-point CTAs
+        const void* fn = nullptr;
+        int C = 0, L = 0, T = 0;
+        if (!cfft_mixc_lookup(P->n, P->dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, &fn, &C, &L, &T))
+            return fail(CFFT_ERR_UNSUPPORTED, "no cluster kernel for n=" + std::to_string(P->n));
+        kp.mode = MODE_MIXC;
+        kp.C = C;
+        kp.N1 = C;
+        kp.N2 = L;
+        rc = make_twolevel(P, L, kp.t4);
+        if (rc) return rc;
+        rc = make_twolevel(P, P->n, kp.t4n);
+        if (rc) return rc;
+        const int nlo = 1 << kp.t4.bits, nhi = (L + nlo - 1) / nlo + 1;
+        const int mlo = 1 << kp.t4n.bits, mhi = (int)((P->n + mlo - 1) / mlo + 1);
+        Stage s;
+        s.kp = kp;
+        s.threads = T;
+        s.smem = (((size_t)L * e + 15) & ~(size_t)15) + (size_t)(nlo + nhi + mlo + mhi) * sizeof(double2);
+        s.cluster = C;
+        s.grid = 0;
+        s.in_sel = 0;
+        s.out_sel = 1;
+        s.fn = fn;
+        CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, C));
+        int nclusters = 0;
+        cudaError_t ce = cfft_max_active_clusters_fn(s.fn, T, s.smem, C, &nclusters);
+        if (ce != cudaSuccess || nclusters < 1) {
+            cudaGetLastError();
+            return fail(CFFT_ERR_UNSUPPORTED, "cluster configuration not schedulable: C=" + std::to_string(C));
+        }
+        s.max_units = nclusters;
+        P->stages.push_back(s);
+        P->chunk = P->batch;
+        return CFFT_OK;
     }
     if (sh.mode == MODE_CONVC) {
         // Rader on C register 4096-point CTAs: permutations in the kernel's
@@ -1299,7 +1357,8 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             unsigned grid;
             if (p2) grid = (unsigned)kp.batch;
             else if (kp.mode == MODE_ROWS) grid = (unsigned)((nb + kp.V - 1) / kp.V);
-            else if (kp.mode == MODE_FOUR || kp.mode == MODE_CONVC) grid = (unsigned)(nb * kp.C);
+            else if (kp.mode == MODE_FOUR || kp.mode == MODE_CONVC || kp.mode == MODE_MIXC)
+                grid = (unsigned)(nb * kp.C);
             else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
             else grid = (unsigned)(nb * (kp.N1 / kp.V));
             if (s.persist && grid > s.persist) grid = s.persist;
@@ -1555,7 +1614,7 @@ static int build_shared_plan(int64_t n, int dtype, int flags, int device, cfft_p
     int rc = fail(CFFT_ERR_UNSUPPORTED, "no execution shape for n=" + std::to_string(n));
     for (auto& c : cands) {
         // not descriptor driven: the batched and served forms skip these
-        if (c.mode == MODE_P2COL || c.mode == MODE_CONVC) continue;
+        if (c.mode == MODE_P2COL || c.mode == MODE_CONVC || c.mode == MODE_MIXC) continue;
         rc = plan_build(P, c);
         if (rc == CFFT_OK) break;
         plan_free(P);

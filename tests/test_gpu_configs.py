@@ -83,15 +83,15 @@ def _bar(ref, x):
 def test_bench_configuration_rows_vs_oracle(cb, n):
     """The benchmarked configuration itself: 1024 transforms of n = 30240
     (mixed radix) or n = 10007 (Rader), forward and inverse, rows 0, 511 and
-    1023 against the oracle; the plans are the benchmark's: the statically
-    shaped four-step cluster kernel for 30240, the cluster of register
-    4096-point CTAs for 10007."""
+    1023 against the oracle; the plans are the benchmark's: a cluster of
+    seven register 4320-point CTAs for 30240, a cluster of five register
+    4096-point CTAs for 10007's convolution."""
     import torch
     batch = 1024
     x = _device_batch(torch, n, batch, np.complex128, seed=n)
     with _CPlan(cb, n, batch, cb.C128) as p:
         desc = p.describe()
-        assert ("+static" in desc) == (n == 30240), desc
+        assert ("cluster(C=7,L=4320" in desc) == (n == 30240), desc
         assert ("rader(n=10007,M=20480)+cluster(C=5" in desc) == (n == 10007), desc
         y = _execute(cb, p.h, x, cb.FORWARD)
         z = _execute(cb, p.h, x, cb.INVERSE)
