@@ -604,6 +604,34 @@ def run_form(args):
     return 0
 
 
+def other_forms(torch, cb, lib, dev, args):
+    """The rest of the metric (plain vs batched / served, p50/p99 at the
+    stated error), measured after the contract line's timed region and
+    attached to it: the power-of-two sweep, the precision form, the batching
+    and serving forms at their configured sizes, and the small-transform
+    latency.  Each summary is the form's own line (python bench.py --form X)
+    without its run bookkeeping; a form that fails records its error."""
+    import copy
+    out = {}
+    for name, fn in (("pow2", form_pow2), ("precision", form_precision), ("batch", form_batch),
+                     ("serve", form_serve), ("small", form_small)):
+        a = copy.copy(args)
+        a.batch, a.exps, a.flag, a.count = 0, "", "none", 20000
+        a.steps = min(args.steps, 20)
+        t0 = time.perf_counter()
+        try:
+            r = fn(torch, cb, lib, dev, a)
+            for k in ("form", "n_gpus", "warmup", "data"):
+                r.pop(k, None)
+        except Exception as exc:                  # recorded, not fatal to the contract line
+            r = {"error": f"{type(exc).__name__}: {exc}"}
+        r["wall_s"] = round(time.perf_counter() - t0, 1)
+        out[name] = r
+        torch.cuda.empty_cache()
+        cb.empty_cache()
+    return out
+
+
 def measure_library(torch, bufs, stream, steps=20):
     """Run-only comparison: torch.fft (cuFFT) on the same resident batches,
     fwd + inv per step.  Not the product; reported for context."""
@@ -644,6 +672,8 @@ def main():
     ap.add_argument("--flag", default="none", choices=("none", "measure"), help="pow2 form: plan flag")
     ap.add_argument("--ref-seconds", type=float, default=60.0,
                     help="reference arm: CPU seconds spread over its warm-up and timed steps")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain form: skip the other forms' summaries appended to the line")
     args = ap.parse_args()
     global SIZES
     if args.only:
@@ -732,7 +762,7 @@ def main():
     n_dom, b_dom, ms_launch, _ = dom
     achieved = 2 * n_dom * b_dom * ELEM / (ms_launch * 1e-3) / 1e9
     peak, peak_kind = load_peaks()
-    traffic = load_traffic().get(f"four_c128_n{n_dom}_b{b_dom}")
+    traffic = load_traffic().get(f"c128_n{n_dom}_b{b_dom}")
 
     e2e = None if args.quick else measure_e2e(torch, cb, lib, plans, bufs, args, world, dev)
     cufft = None if args.quick else measure_library(torch, bufs, stream)
@@ -745,8 +775,19 @@ def main():
                "sample": f"{res[2]} units (fwd+inv of one 30240 and one 10007 transform) in "
                          f"{res[1]:.1f} s, OpenMP over {threads} threads"}
 
+    descs = []
     for h in plans:
+        d = ctypes.create_string_buffer(256)
+        lib.cfft_plan_describe(h, d, 256)
+        descs.append(d.value.decode())
         lib.cfft_plan_destroy(h)
+    dom_desc = descs[[n for n, _ in SIZES].index(n_dom)]
+    forms = None
+    if rank == 0 and world == 1 and not args.quick and not args.no_forms:
+        del bufs
+        torch.cuda.empty_cache()
+        cb.empty_cache()
+        forms = other_forms(torch, cb, lib, dev, args)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
@@ -760,13 +801,16 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": f"k_four<double2> n={n_dom} batch={b_dom}",
+                         "kernel": f"n={n_dom} batch={b_dom}: {dom_desc}",
                          "ms_per_launch": round(ms_launch, 4)},
             "per_size_ms_per_launch": {str(n): round(m, 4) for n, _, m, _ in per},
+            "plans": {str(n): d for (n, _), d in zip(SIZES, descs)},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "library_comparison": cufft,
             "clocks": clk.summary(),
         }
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line))
     if world > 1:
         torch.distributed.barrier()
