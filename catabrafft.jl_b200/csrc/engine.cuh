@@ -293,6 +293,35 @@ template <typename V>
 __device__ __forceinline__ V r4096_tw(V v, const double2* lo, const double2* hi, unsigned e) {
     return e ? cmul(v, fromd<V>(r4096_w(lo, hi, e))) : v;
 }
+// 4096-point DFT of the registers: thread t holds x[t + 256 k] in v[k] and
+// gets X[t + 256 k3] in v[k3].  buf (16 planes of R4096_PL elements) must be
+// free on entry; on return every thread has finished reading it.
+template <typename V>
+__device__ __forceinline__ void fft4096_regs(V (&v)[16], V* buf, const double2* tlo, const double2* thi, int t) {
+    dft<16>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = r4096_tw(v[k1], tlo, thi, (unsigned)(t * k1));
+    __syncthreads();
+    {
+        const int t1 = t & 15, k1 = t >> 4;
+#pragma unroll
+        for (int t2 = 0; t2 < 16; t2++) v[t2] = buf[k1 * 256 + t1 + 16 * t2];
+        dft<16>(v);
+        __syncthreads();                        // every Y read before Z overwrites it
+#pragma unroll
+        for (int k2 = 0; k2 < 16; k2++)
+            buf[k1 * R4096_PL + k2 * R4096_PB + t1] = r4096_tw(v[k2], tlo, thi, (unsigned)(16 * t1 * k2));
+    }
+    __syncthreads();
+    {
+        const int k1 = t & 15, k2 = t >> 4;
+#pragma unroll
+        for (int t1 = 0; t1 < 16; t1++) v[t1] = buf[k1 * R4096_PL + k2 * R4096_PB + t1];
+    }
+    __syncthreads();                            // every Z read: the buffer is free
+    dft<16>(v);
+}
+
 // Persistent: CTA g transforms g, g + gridDim.x, ...  A thread's input
 // elements x[t + 256 k] are copied by cp.async to buf[t + 256 k], exactly
 // where the same thread later reads them and writes its Y values, so the

@@ -31,7 +31,7 @@ struct TwoLevel {                 // w_N^e = lo[e & mask] * hi[e >> bits]  (FP64
 };
 
 enum { MODE_ROWS = 0, MODE_FOUR = 1, MODE_COLPASS = 2, MODE_ROWPASS = 3, MODE_P2COL = 4, MODE_P2ROW = 5,
-       MODE_CONVC = 6, MODE_MIXC = 7 };
+       MODE_CONVC = 6, MODE_MIXC = 7, MODE_P2CL = 8 };
 // kernel selector only (KParams.mode stays MODE_FOUR): the generic four-step
 // kernel instantiated with warp-synchronous sub-transforms
 enum { MODE_FOUR_WARP = 16 };

@@ -191,6 +191,25 @@ const void* cfft_p2col_kernel(int dtype, int N1, int mb) {
     if (dtype == CFFT_DT_C128) return mb == 2 ? p2col_for<double2, 2>(N1) : p2col_for<double2, 3>(N1);
     return p2col_for<float2, 3>(N1);
 }
+// single-pass power-of-two n = C x 4096 on clusters of C CTAs (pow2.cuh)
+template <typename V, int C, int MB>
+__global__ void __launch_bounds__(CFFT_THREADS, MB) k_p2cl(KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    p2cl_body<V, C>(p, smem);
+}
+template <typename V, int MB> static const void* p2cl_for(int C) {
+    switch (C) {
+        case 2: return (const void*)k_p2cl<V, 2, MB>;
+        case 4: return (const void*)k_p2cl<V, 4, MB>;
+        case 8: return (const void*)k_p2cl<V, 8, MB>;
+        case 16: return (const void*)k_p2cl<V, 16, MB>;
+    }
+    return nullptr;
+}
+const void* cfft_p2cl_kernel(int dtype, int C, int mb) {
+    if (dtype == CFFT_DT_C128) return mb == 2 ? p2cl_for<double2, 2>(C) : p2cl_for<double2, 3>(C);
+    return mb == 2 ? p2cl_for<float2, 2>(C) : p2cl_for<float2, 3>(C);
+}
 const void* cfft_p2row_tma_kernel(int mb) {
     return mb == 2 ? (const void*)k_p2row_tma<2> : (const void*)k_p2row_tma<3>;
 }
@@ -278,25 +297,28 @@ size_t cfft_convc_smem(size_t elem_bytes) {
 }
 
 // mixed-radix lengths n = C L on a cluster of C register L-point CTAs
-// (mixc.cuh), two CTAs per SM
-template <typename V, class S>
-__global__ void __launch_bounds__(S::T, 2) k_mixc(KParams p) {
+// (mixc.cuh): two CTAs per SM with both tables staged, or three with the
+// w_n table read through L2 (variant 1; ComplexF64 spills at that budget)
+template <typename V, class S, int MB, bool GTAB>
+__global__ void __launch_bounds__(S::T, MB) k_mixc(KParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
-    mixc_body<V, S>(p, smem);
+    mixc_body<V, S, GTAB>(p, smem);
 }
 struct MixEntry {
     int n, C, L, threads;
-    const void* fn[2];            // ComplexF64, ComplexF32
+    const void* fn[2][2];         // [variant][ComplexF64, ComplexF32]
 };
 // 30240 = 7 x 4320, 4320 = 16 x 18 x 15 (the mixed-radix benchmark length)
 using Mix30240 = MixShape<7, 16, 18, 15, 288>;
 static const MixEntry kMix[] = {
-    {30240, 7, 4320, 288, {(const void*)k_mixc<double2, Mix30240>, (const void*)k_mixc<float2, Mix30240>}},
+    {30240, 7, 4320, 288,
+     {{(const void*)k_mixc<double2, Mix30240, 2, false>, (const void*)k_mixc<float2, Mix30240, 2, false>},
+      {(const void*)k_mixc<double2, Mix30240, 3, true>, (const void*)k_mixc<float2, Mix30240, 3, true>}}},
 };
-int cfft_mixc_lookup(long long n, int dtype, const void** fn, int* C, int* L, int* threads) {
+int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads) {
     for (const auto& m : kMix) {
-        if (m.n != n) continue;
-        *fn = m.fn[dtype == CFFT_DT_C128 ? 0 : 1];
+        if (m.n != n || variant < 0 || variant > 1) continue;
+        *fn = m.fn[variant][dtype == CFFT_DT_C128 ? 0 : 1];
         *C = m.C;
         *L = m.L;
         *threads = m.threads;

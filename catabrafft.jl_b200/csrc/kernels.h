@@ -29,6 +29,10 @@ size_t cfft_r4096_smem(size_t elem_bytes);
 // memory cfft_p2col_smem), built for mb = 3 or 2 CTAs per SM (ComplexF64;
 // ComplexF32 is always 3)
 const void* cfft_p2col_kernel(int dtype, int N1, int mb);
+// single-pass power-of-two n = C x 4096 (C in {2, 4, 8, 16}) on clusters of C
+// register 4096-point CTAs, mb = 2 or 3 CTAs per SM; shared memory
+// cfft_r4096_smem
+const void* cfft_p2cl_kernel(int dtype, int C, int mb);
 // pass A with tensor copies (ComplexF64), and its launcher (encodes the
 // tensor map of p.in for this launch)
 const void* cfft_p2row_tma_kernel(int mb);
@@ -39,8 +43,10 @@ cudaError_t cfft_launch_p2row_tma(const void* fn, const KParams& p, unsigned gri
 const void* cfft_convc_kernel(int dtype, int C, int mb);
 size_t cfft_convc_smem(size_t elem_bytes);
 // mixed-radix lengths with a cluster kernel of C register L-point CTAs
-// (mixc.cuh): 1 and the kernel, C, L and threads per CTA, else 0
-int cfft_mixc_lookup(long long n, int dtype, const void** fn, int* C, int* L, int* threads);
+// (mixc.cuh): 1 and the kernel, C, L and threads per CTA, else 0; variant 0
+// stages both twiddle tables (two CTAs per SM), variant 1 reads the w_n
+// table through L2 (three CTAs per SM)
+int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads);
 // the device fault word (bit 0: a tensor-copy wait timed out), optionally cleared
 cudaError_t cfft_device_fault_word(unsigned* out, int clear);
 const void* cfft_p2row_kernel(int dtype, int mb);

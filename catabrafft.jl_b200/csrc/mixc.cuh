@@ -48,9 +48,11 @@ __device__ __forceinline__ V mx_tw(V v, const double2* lo, const double2* hi, in
 }
 
 // KParams: t4 = two-level table of w_L, t4n = two-level table of w_n (both
-// staged in shared memory after the buffer), in / out at in_dist / out_dist,
-// batch = transforms (one per cluster).
-template <typename V, class S>
+// staged in shared memory after the buffer unless GTAB), in / out at
+// in_dist / out_dist, batch = transforms (one per cluster).
+// GTAB: the w_n table is read through L2 instead of being staged (frees
+// its shared memory for a third CTA per SM)
+template <typename V, class S, bool GTAB = false>
 __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem) {
     cg::cluster_group cl = cg::this_cluster();
     const int c = (int)cl.block_rank();
@@ -61,7 +63,8 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
     const int bl = p.t4.bits, bn = p.t4n.bits;
     const int nlo = 1 << bl, nhi = (p.t4.N + nlo - 1) / nlo + 1;
     const int mlo = 1 << bn, mhi = (p.t4n.N + mlo - 1) / mlo + 1;
-    double2 *llo = tab, *lhi = tab + nlo, *glo = lhi + nhi, *ghi = glo + mlo;
+    double2 *llo = tab, *lhi = tab + nlo;
+    const double2 *glo = GTAB ? p.t4n.lo : lhi + nhi, *ghi = GTAB ? p.t4n.hi : lhi + nhi + mlo;
     {
         // stage-0 inputs: thread b < NB0 owns slots b + NB0 m = x[c + C (b + NB0 m)]
         const int b = opaque_tid();
@@ -72,7 +75,10 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
         }
         cp_async_commit();
         for (int i = b; i < nlo + nhi; i += S::T) tab[i] = (i < nlo) ? p.t4.lo[i] : p.t4.hi[i - nlo];
-        for (int i = b; i < mlo + mhi; i += S::T) glo[i] = (i < mlo) ? p.t4n.lo[i] : p.t4n.hi[i - mlo];
+        if (!GTAB) {
+            double2* gs = lhi + nhi;
+            for (int i = b; i < mlo + mhi; i += S::T) gs[i] = (i < mlo) ? p.t4n.lo[i] : p.t4n.hi[i - mlo];
+        }
     }
     V v[S::RMAX];
     {

@@ -483,6 +483,28 @@ static void conv_kind(int64_t n, int& conv, int64_t& M) {
 // (pow2.cuh); V carries the CTAs per SM the kernels are built for
 static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     if (n < 8192 || n > (1 << 22) || (n & (n - 1))) return;
+    // up to 2^16: one pass on a cluster of n / 4096 register 4096-point CTAs.
+    // Measured on B200 (1 GiB batches, ComplexF64): 8192 0.64 ms and 16384
+    // 0.82 ms against 0.99 / 1.00 for the two passes; at 32768 and 65536 the
+    // 8- and 16-CTA clusters fit only 33 / 14 at a time and lose (1.15 / 1.62
+    // against 0.92 / 0.93 ms), so there they follow the two-pass shapes
+    std::vector<Shape> cl;
+    if (n <= 65536) {
+        for (int mb : {2, 3}) {
+            Shape s;
+            s.mode = MODE_P2CL;
+            s.conv = CONV_NONE;
+            s.M = n;
+            s.N1 = (int)(n / 4096);
+            s.N2 = 4096;
+            s.C = (int)(n / 4096);
+            s.V = mb;
+            s.rc = {16, 16, 16};
+            cl.push_back(s);
+        }
+    }
+    const bool cluster_first = n <= 16384;
+    if (cluster_first) out.insert(out.end(), cl.begin(), cl.end());
     // V = CTAs per SM of pass A (the n = 4096 kernel over strided rows):
     // three like the n = 4096 plan, or two (no spills) for ComplexF64;
     // ComplexF64 pass A by tensor copies (var = 1) first from N1 = 8 (one
@@ -504,6 +526,7 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
         s.rc = {16, 16, 16};
         out.push_back(s);
     }
+    if (!cluster_first) out.insert(out.end(), cl.begin(), cl.end());
 }
 
 // primes above 4096: Rader's convolution on a cluster of C register
@@ -534,18 +557,26 @@ static void convc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
 // mixed-radix lengths with a cluster kernel of register L-point CTAs
 // (mixc.cuh): n = C x L
 static void mixc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
-    const void* fn = nullptr;
-    int C = 0, L = 0, T = 0;
-    if (!cfft_mixc_lookup(n, dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, &fn, &C, &L, &T)) return;
-    Shape s;
-    s.mode = MODE_MIXC;
-    s.conv = CONV_NONE;
-    s.M = n;
-    s.N1 = C;
-    s.N2 = L;
-    s.C = C;
-    s.V = T;
-    out.push_back(s);
+    // measured on B200 (1024 x 30240): ComplexF64 0.594 ms with both tables
+    // staged at two CTAs per SM against 0.635 at three (which spills);
+    // ComplexF32 0.367 ms at three against 0.456 at two
+    const bool three_first = dtype != CFFT_C128;
+    for (int i = 0; i < 2; i++) {
+        const int var = three_first ? 1 - i : i;
+        const void* fn = nullptr;
+        int C = 0, L = 0, T = 0;
+        if (!cfft_mixc_lookup(n, dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, var, &fn, &C, &L, &T)) return;
+        Shape s;
+        s.mode = MODE_MIXC;
+        s.conv = CONV_NONE;
+        s.M = n;
+        s.N1 = C;
+        s.N2 = L;
+        s.C = C;
+        s.V = T;
+        s.var = var;
+        out.push_back(s);
+    }
 }
 
 static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) {
@@ -599,9 +630,11 @@ static std::string shape_desc(const Shape& s, int64_t n) {
     std::string pre = c.empty() ? "" : c + "(n=" + std::to_string(n) + ",M=" + std::to_string(s.M) + ")+";
     if (s.mode == MODE_ROWS)
         return pre + "rows(V=" + std::to_string(s.V) + ")[" + join(s.rc) + "]";
+    if (s.mode == MODE_P2CL)
+        return "pow2cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_MIXC)
         return "cluster(C=" + std::to_string(s.C) + ",L=" + std::to_string(s.N2) + " per CTA,threads=" +
-               std::to_string(s.V) + ")";
+               std::to_string(s.V) + (s.var == 1 ? ",ctas_per_sm=3" : "") + ")";
     if (s.mode == MODE_CONVC)
         return pre + "cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_P2COL)
@@ -944,11 +977,41 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
             kp.spec = (const double2*)d;
         }
     }
+    if (sh.mode == MODE_P2CL) {
+        // power-of-two n = C x 4096 in one pass on clusters of C CTAs
+        kp.mode = MODE_P2CL;
+        kp.C = sh.C;
+        rc = make_twolevel(P, 4096, kp.t4);
+        if (rc) return rc;
+        rc = make_twolevel(P, P->n, kp.t4n);
+        if (rc) return rc;
+        Stage s;
+        s.kp = kp;
+        s.threads = CFFT_THREADS;
+        s.smem = cfft_r4096_smem(e);
+        s.cluster = sh.C;
+        s.grid = 0;
+        s.in_sel = 0;
+        s.out_sel = 1;
+        s.fn = cfft_p2cl_kernel(P->dtype, sh.C, sh.V);
+        if (!s.fn) return fail(CFFT_ERR_UNSUPPORTED, "no power-of-two cluster kernel for C=" + std::to_string(sh.C));
+        CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, sh.C));
+        int nclusters = 0;
+        cudaError_t ce = cfft_max_active_clusters_fn(s.fn, CFFT_THREADS, s.smem, sh.C, &nclusters);
+        if (ce != cudaSuccess || nclusters < 1) {
+            cudaGetLastError();
+            return fail(CFFT_ERR_UNSUPPORTED, "cluster configuration not schedulable: C=" + std::to_string(sh.C));
+        }
+        s.max_units = nclusters;
+        P->stages.push_back(s);
+        P->chunk = P->batch;
+        return CFFT_OK;
+    }
     if (sh.mode == MODE_MIXC) {
         // n = C x L on a cluster of C register L-point CTAs
         const void* fn = nullptr;
         int C = 0, L = 0, T = 0;
-        if (!cfft_mixc_lookup(P->n, P->dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, &fn, &C, &L, &T))
+        if (!cfft_mixc_lookup(P->n, P->dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, sh.var, &fn, &C, &L, &T))
             return fail(CFFT_ERR_UNSUPPORTED, "no cluster kernel for n=" + std::to_string(P->n));
         kp.mode = MODE_MIXC;
         kp.C = C;
@@ -963,7 +1026,8 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         Stage s;
         s.kp = kp;
         s.threads = T;
-        s.smem = (((size_t)L * e + 15) & ~(size_t)15) + (size_t)(nlo + nhi + mlo + mhi) * sizeof(double2);
+        s.smem = (((size_t)L * e + 15) & ~(size_t)15) +
+                 (size_t)(nlo + nhi + (sh.var == 1 ? 0 : mlo + mhi)) * sizeof(double2);
         s.cluster = C;
         s.grid = 0;
         s.in_sel = 0;
@@ -1357,7 +1421,7 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             unsigned grid;
             if (p2) grid = (unsigned)kp.batch;
             else if (kp.mode == MODE_ROWS) grid = (unsigned)((nb + kp.V - 1) / kp.V);
-            else if (kp.mode == MODE_FOUR || kp.mode == MODE_CONVC || kp.mode == MODE_MIXC)
+            else if (kp.mode == MODE_FOUR || kp.mode == MODE_CONVC || kp.mode == MODE_MIXC || kp.mode == MODE_P2CL)
                 grid = (unsigned)(nb * kp.C);
             else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
             else grid = (unsigned)(nb * (kp.N1 / kp.V));
@@ -1614,7 +1678,7 @@ static int build_shared_plan(int64_t n, int dtype, int flags, int device, cfft_p
     int rc = fail(CFFT_ERR_UNSUPPORTED, "no execution shape for n=" + std::to_string(n));
     for (auto& c : cands) {
         // not descriptor driven: the batched and served forms skip these
-        if (c.mode == MODE_P2COL || c.mode == MODE_CONVC || c.mode == MODE_MIXC) continue;
+        if (c.mode == MODE_P2COL || c.mode == MODE_CONVC || c.mode == MODE_MIXC || c.mode == MODE_P2CL) continue;
         rc = plan_build(P, c);
         if (rc == CFFT_OK) break;
         plan_free(P);

@@ -264,3 +264,62 @@ __device__ __forceinline__ void p2col_body(const KParams& p, unsigned char* smem
         }
     }
 }
+
+// ------------------------------------------------------------------------
+// Single pass for n = C x 4096, C in {2, 4, 8, 16}: a cluster of C CTAs per
+// transform.  CTA c loads the stride-C subsequence x[c + C t], t < 4096, into
+// registers, transforms it with the register 4096-point FFT (fft4096_regs)
+// and publishes F_c[k] in shared memory; after one cluster barrier the
+// cluster's threads take k round robin and combine
+//   X[k + 4096 q] = sum_c w_n^(c k) F_c[k] w_C^(c q)
+// through distributed shared memory, storing whole segments for each q.  The
+// data crosses HBM once (the two-pass form writes and reads an
+// intermediate).  KParams: t4 = two-level table of w_4096 (staged), t4n =
+// two-level table of w_n (read through L2), batch = transforms.
+template <typename V, int C>
+__device__ __forceinline__ void p2cl_body(const KParams& p, unsigned char* smem) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int c = (int)cl.block_rank();
+    const int tr = block_id(p) / C;
+    if (tr >= p.batch) return;                  // uniform across the cluster
+    V* buf = (V*)smem;                          // 16 planes of R4096_PL elements
+    double2* tlo = after16(buf + 16 * R4096_PL);
+    double2* thi = tlo + 64;
+    V v[16];
+    {
+        const int t = opaque_tid();
+        if (t < 64) tlo[t ^ (t >> 3)] = p.t4.lo[t];
+        if (t < 65) thi[t] = p.t4.hi[t];
+        const V* x = (const V*)p.in + (long long)tr * p.in_dist + c + (long long)C * t;
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] = load_in(p, __ldg(x + (long long)C * 256 * k));
+    }
+    __syncthreads();                            // tables staged
+    fft4096_regs(v, buf, tlo, thi, opaque_tid());
+    {
+        const int t = opaque_tid();
+#pragma unroll
+        for (int k3 = 0; k3 < 16; k3++) buf[t + 256 * k3] = v[k3];
+    }
+    cl.sync();                                  // every F_c published
+    {
+        const int g = c * 256 + opaque_tid();
+        V* out = (V*)p.out + (long long)tr * p.out_dist;
+        const unsigned mask = (1u << p.t4n.bits) - 1;
+#pragma unroll 1
+        for (int k = g; k < 4096; k += C * 256) {
+            V f[C];
+#pragma unroll
+            for (int q = 0; q < C; q++) f[q] = cl.map_shared_rank(buf, q)[k];
+#pragma unroll
+            for (int q = 1; q < C; q++) {
+                const unsigned e = (unsigned)(q * k);
+                f[q] = cmul(f[q], fromd<V>(cmul(__ldg(p.t4n.lo + (e & mask)), __ldg(p.t4n.hi + (e >> p.t4n.bits)))));
+            }
+            dft<C>(f);
+#pragma unroll
+            for (int q = 0; q < C; q++) stg_stream(out + k + 4096 * q, store_out(p, f[q]));
+        }
+    }
+    cl.sync();                                  // no CTA leaves while a peer reads its F
+}

@@ -197,7 +197,8 @@ def _pow2_check(cb, n, batch, dtype, desc_part, flags=0):
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
 def test_pow2_register_passes(cb, dtype):
-    """Power-of-two n = N1 x 4096 (N1 = 2 .. 1024): pass A (the n = 4096
+    """Power-of-two n = N1 x 4096 (N1 = 2 .. 1024): up to 2^16 one pass on a
+    cluster of N1 register 4096-point CTAs; beyond, pass A (the n = 4096
     kernel over the stride-N1 subsequences; ComplexF64 loads them by tensor
     copies) and pass B (the N1-point column DFTs).  Batches give every
     persistent CTA several rows and tiles (prefetch into the freed buffer),
@@ -209,8 +210,11 @@ def test_pow2_register_passes(cb, dtype):
         n = 1 << e
         N1 = n // 4096
         batch = max(3, 2048 // N1 + 1)
-        tag = ",tma)" if dtype == np.complex128 and N1 >= 8 else ")"
-        _pow2_check(cb, n, batch, dtype, f"pow2(N1={N1},N2=4096,ctas_per_sm=3{tag}")
+        if n <= 16384:                              # one pass on a cluster of N1 CTAs
+            _pow2_check(cb, n, batch, dtype, f"pow2cluster(C={N1},4096 per CTA,ctas_per_sm=2)")
+        else:
+            tag = ",tma)" if dtype == np.complex128 else ")"
+            _pow2_check(cb, n, batch, dtype, f"pow2(N1={N1},N2=4096,ctas_per_sm=3{tag}")
     assert cb._lib.LIB.cfft_device_faults(1) == 0
 
 
@@ -219,7 +223,7 @@ def test_pow2_other_variants(cb, tmp_path):
     MEASURE plans: cp.async loads and tensor copies, at three and at two CTAs
     per SM."""
     variants = [(3, 0, ")"), (2, 0, ")"), (3, 1, ",tma)"), (2, 1, ",tma)")]
-    cases = [(1 << 13, 300), (1 << 16, 40), (1 << 20, 3), (1 << 22, 9)]
+    cases = [(1 << 13, 300), (1 << 14, 150), (1 << 15, 80), (1 << 16, 40), (1 << 20, 3), (1 << 22, 9)]
     cb._lib.LIB.cfft_device_faults(1)
     for mb, var, tag in variants:
         lines = ["catabra-b200-wisdom 1"]
@@ -240,3 +244,38 @@ def test_pow2_other_variants(cb, tmp_path):
         finally:
             cb.forget_wisdom()
     assert cb._lib.LIB.cfft_device_faults(1) == 0
+
+
+def test_pow2_cluster_three_ctas_per_sm(cb, tmp_path):
+    """The single-pass cluster kernels not chosen by default, reached through
+    wisdom entries for MEASURE plans, both element types: three CTAs per SM
+    for every C, and two CTAs per SM for the 8- and 16-CTA clusters."""
+    cases = [(1 << 13, 300, 3), (1 << 14, 150, 3), (1 << 15, 80, 3), (1 << 16, 40, 3), (1 << 15, 80, 2),
+             (1 << 16, 40, 2)]
+    for dtype, code in ((np.complex128, 0), (np.complex64, 1)):
+        lines = ["catabra-b200-wisdom 1"]
+        for n, batch, mb in cases[:4]:
+            C = n // 4096
+            lines.append(f"{n} {batch} {code} {cb.MEASURE} | 8 0 {n} {C} 4096 {C} {mb} a c 16 16 16")
+        path = tmp_path / f"c{code}.txt"
+        path.write_text("\n".join(lines) + "\n")
+        cb.forget_wisdom()
+        cb.import_wisdom(str(path))
+        try:
+            for n, batch, mb in cases[:4]:
+                _pow2_check(cb, n, batch, dtype, f"pow2cluster(C={n // 4096},4096 per CTA,ctas_per_sm={mb})",
+                            flags=cb.MEASURE)
+        finally:
+            cb.forget_wisdom()
+        lines = ["catabra-b200-wisdom 1"]
+        for n, batch, mb in cases[4:]:
+            C = n // 4096
+            lines.append(f"{n} {batch} {code} {cb.MEASURE} | 8 0 {n} {C} 4096 {C} {mb} a c 16 16 16")
+        path.write_text("\n".join(lines) + "\n")
+        cb.import_wisdom(str(path))
+        try:
+            for n, batch, mb in cases[4:]:
+                _pow2_check(cb, n, batch, dtype, f"pow2cluster(C={n // 4096},4096 per CTA,ctas_per_sm={mb})",
+                            flags=cb.MEASURE)
+        finally:
+            cb.forget_wisdom()
