@@ -58,6 +58,7 @@ SIGNATURES = {
     "cfft_wisdom_entries": (_i64, []),
     "cfft_debug_alloc_hook": (_i64, [_i64]),
     "cfft_device_faults": (_ci, [_ci]),
+    "cfft_debug_wait_timeout": (_ci, [_ci]),
 }
 
 

@@ -253,6 +253,23 @@ cudaError_t cfft_launch_p2row_tma(const void* f, const KParams& p, unsigned grid
     if (e != cudaSuccess) cudaGetLastError();
     return e;
 }
+// The timeout path of the bounded waits, exercised without a fault: one
+// thread arms nothing and waits on a fresh mbarrier's phase 0, which no one
+// completes; after `polls` polls the wait gives up and records the fault bit
+// exactly as a kernel whose tensor copy never landed would.
+__global__ void k_wait_probe(int polls) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        if (!mbar_wait(&bar, 0, polls)) record_fault(kFaultTmaTimeout);
+    }
+}
+cudaError_t cfft_wait_probe(int polls) {
+    k_wait_probe<<<1, 32>>>(polls);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e;
+}
 cudaError_t cfft_device_fault_word(unsigned* out, int clear) {
     cudaError_t e = cudaMemcpyFromSymbol(out, g_cfft_fault, sizeof(unsigned));
     if (e == cudaSuccess && clear) {

@@ -47,6 +47,9 @@ size_t cfft_convc_smem(size_t elem_bytes);
 // stages both twiddle tables (two CTAs per SM), variant 1 reads the w_n
 // table through L2 (three CTAs per SM)
 int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads);
+// launch a one-thread kernel whose bounded wait (at most `polls` polls) runs
+// out on an mbarrier no one completes, and wait for it
+cudaError_t cfft_wait_probe(int polls);
 // the device fault word (bit 0: a tensor-copy wait timed out), optionally cleared
 cudaError_t cfft_device_fault_word(unsigned* out, int clear);
 const void* cfft_p2row_kernel(int dtype, int mb);

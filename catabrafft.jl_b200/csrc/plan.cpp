@@ -2319,6 +2319,12 @@ int cfft_device_faults(int clear) {
     return (int)w;
 }
 
+int cfft_debug_wait_timeout(int polls) {
+    if (polls < 1 || polls > (1 << 20)) return fail(CFFT_ERR_INVALID, "polls must be in [1, 2^20]");
+    CUDA_TRY(cfft_wait_probe(polls));
+    return CFFT_OK;
+}
+
 int64_t cfft_debug_alloc_hook(int64_t nth) {
     g_alloc_seq.store(0);
     g_alloc_fail_from.store(nth > 0 ? nth : 0);

@@ -34,10 +34,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
-// true once the barrier's phase `parity` has completed; false after the limit
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// true once the barrier's phase `parity` has completed; false after `limit`
+// polls (kWaitLimit unless a caller asks for fewer)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit = kWaitLimit) {
     const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < kWaitLimit; it++) {
+    for (int it = 0; it < limit; it++) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

@@ -228,6 +228,13 @@ int cfft_fft_twopass_noalloc(int64_t n, int64_t batch, int dtype, const void* d_
  * it could not be read (cfft_last_error() has the reason). */
 int cfft_device_faults(int clear);
 
+/* Test hook, no counterpart in the reference.  Runs a one-thread kernel whose
+ * bounded wait (at most `polls` polls, 1 .. 2^20) on an mbarrier that nothing
+ * completes gives up, and waits for it: the same timeout path a kernel takes
+ * when its tensor copies never land, exercised without any fault.  Afterwards
+ * cfft_device_faults reports bit 0 and the context stays usable. */
+int cfft_debug_wait_timeout(int polls);
+
 /* Test hook, no counterpart in the reference (whose failures are Julia
  * exceptions from @assert / error, src/kernel.jl:113,187, src/prime.jl:6,27,43).
  * From the nth device or pinned host allocation the library makes after this

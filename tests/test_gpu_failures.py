@@ -1,4 +1,5 @@
-"""Failure paths on the host side: allocations that fail as out of memory.
+"""Failure paths: allocations that fail as out of memory, and a device-side
+wait that runs out.
 
 The reference has no failure handling beyond Julia exceptions
 (src/kernel.jl:113,187; src/prime.jl:6,27,43).  Here every create entry
@@ -8,6 +9,9 @@ the host (cfft_debug_alloc_hook makes the library's own allocations report
 out-of-memory from the nth on); nothing faults the device.  A leak shows as
 a live-allocation count (the library counts its own device and pinned host
 allocations) or free device memory that does not return to its baseline.
+The kernels' bounded waits are exercised on an mbarrier that nothing
+completes (cfft_debug_wait_timeout): the wait gives up, the device fault
+word reports it, and the context stays usable.
 """
 import ctypes
 
@@ -179,3 +183,19 @@ def test_empty_cache_while_server_is_live(cb):
         bar = max(1e-12, np.linalg.norm(ref - np.fft.fft(v)) / np.linalg.norm(ref) + 1e-12)
         assert np.linalg.norm(a.cpu().numpy() - ref) / np.linalg.norm(ref) < bar
         assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+
+
+def test_bounded_wait_times_out_without_a_fault(cb):
+    """A kernel's bounded wait on an mbarrier that nothing completes gives up
+    after its poll limit, records the device fault bit and returns: the host
+    reads the bit, clears it, and the context keeps working."""
+    lib = cb._lib.LIB
+    assert lib.cfft_device_faults(1) >= 0
+    assert lib.cfft_device_faults(0) == 0
+    cb.check(lib.cfft_debug_wait_timeout(1000))
+    assert lib.cfft_device_faults(1) & 1
+    assert lib.cfft_device_faults(0) == 0
+    x = np.ones(4096, dtype=np.complex128)
+    assert abs(cb.fft(x)[0] - 4096) < 1e-9                # the context is still usable
+    with pytest.raises(cb.CatabraError):
+        cb.check(lib.cfft_debug_wait_timeout(0))
