@@ -114,6 +114,10 @@ export_wisdom(path::AbstractString) = check(ccall((:cfft_wisdom_export, LIB), Ci
 import_wisdom(path::AbstractString) = check(ccall((:cfft_wisdom_import, LIB), Cint, (Cstring,), path))
 forget_wisdom() = check(ccall((:cfft_wisdom_forget, LIB), Cint, ()))
 
+# the device fault word: 0 unless a kernel's bounded wait on its tensor
+# copies gave up (that launch's results are then incomplete)
+device_faults(clear::Bool = false) = ccall((:cfft_device_faults, LIB), Cint, (Cint,), clear ? 1 : 0)
+
 function empty_cache()
     for p in values(PLANS)
         finalize(p)
