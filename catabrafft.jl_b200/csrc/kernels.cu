@@ -323,19 +323,25 @@ __global__ void __launch_bounds__(S::T, MB) k_mixc(KParams p) {
 }
 struct MixEntry {
     int n, C, L, threads;
-    const void* fn[2][2];         // [variant][ComplexF64, ComplexF32]
+    const void* fn[2];            // ComplexF64, ComplexF32
 };
-// 30240 = 7 x 4320, 4320 = 16 x 18 x 15 (the mixed-radix benchmark length)
+// 30240 = 7 x 4320, 4320 = 16 x 18 x 15 on 288 threads (variants 0, 1), and
+// 30240 = 9 x 3360, 3360 = 14 x 16 x 15 on 240 threads (variants 2 and 3:
+// the stages keep 240 / 210 / 224 of 240 threads busy, 16 values per thread
+// at most; three or two CTAs per SM)
 using Mix30240 = MixShape<7, 16, 18, 15, 288>;
-static const MixEntry kMix[] = {
-    {30240, 7, 4320, 288,
-     {{(const void*)k_mixc<double2, Mix30240, 2, false>, (const void*)k_mixc<float2, Mix30240, 2, false>},
-      {(const void*)k_mixc<double2, Mix30240, 3, true>, (const void*)k_mixc<float2, Mix30240, 3, true>}}},
+using Mix30240b = MixShape<9, 14, 16, 15, 240>;
+static const MixEntry kMix[][4] = {
+    {{30240, 7, 4320, 288, {(const void*)k_mixc<double2, Mix30240, 2, false>, (const void*)k_mixc<float2, Mix30240, 2, false>}},
+     {30240, 7, 4320, 288, {(const void*)k_mixc<double2, Mix30240, 3, true>, (const void*)k_mixc<float2, Mix30240, 3, true>}},
+     {30240, 9, 3360, 240, {(const void*)k_mixc<double2, Mix30240b, 3, false>, (const void*)k_mixc<float2, Mix30240b, 3, false>}},
+     {30240, 9, 3360, 240, {(const void*)k_mixc<double2, Mix30240b, 2, false>, (const void*)k_mixc<float2, Mix30240b, 2, false>}}},
 };
 int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads) {
-    for (const auto& m : kMix) {
-        if (m.n != n || variant < 0 || variant > 1) continue;
-        *fn = m.fn[variant][dtype == CFFT_DT_C128 ? 0 : 1];
+    for (const auto& row : kMix) {
+        if (row[0].n != n || variant < 0 || variant > 3) continue;
+        const MixEntry& m = row[variant];
+        *fn = m.fn[dtype == CFFT_DT_C128 ? 0 : 1];
         *C = m.C;
         *L = m.L;
         *threads = m.threads;

@@ -45,7 +45,8 @@ size_t cfft_convc_smem(size_t elem_bytes);
 // mixed-radix lengths with a cluster kernel of C register L-point CTAs
 // (mixc.cuh): 1 and the kernel, C, L and threads per CTA, else 0; variant 0
 // stages both twiddle tables (two CTAs per SM), variant 1 reads the w_n
-// table through L2 (three CTAs per SM)
+// table through L2 (three CTAs per SM), variants 2 and 3 are another split
+// of n at three and two CTAs per SM
 int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads);
 // launch a one-thread kernel whose bounded wait (at most `polls` polls) runs
 // out on an mbarrier no one completes, and wait for it

@@ -561,8 +561,8 @@ static void mixc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     // staged at two CTAs per SM against 0.635 at three (which spills);
     // ComplexF32 0.367 ms at three against 0.456 at two
     const bool three_first = dtype != CFFT_C128;
-    for (int i = 0; i < 2; i++) {
-        const int var = three_first ? 1 - i : i;
+    for (int i = 0; i < 4; i++) {
+        const int var = i >= 2 ? i : (three_first ? 1 - i : i);
         const void* fn = nullptr;
         int C = 0, L = 0, T = 0;
         if (!cfft_mixc_lookup(n, dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, var, &fn, &C, &L, &T)) return;
@@ -634,7 +634,7 @@ static std::string shape_desc(const Shape& s, int64_t n) {
         return "pow2cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_MIXC)
         return "cluster(C=" + std::to_string(s.C) + ",L=" + std::to_string(s.N2) + " per CTA,threads=" +
-               std::to_string(s.V) + (s.var == 1 ? ",ctas_per_sm=3" : "") + ")";
+               std::to_string(s.V) + (s.var == 1 || s.var == 2 ? ",ctas_per_sm=3" : "") + ")";
     if (s.mode == MODE_CONVC)
         return pre + "cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_P2COL)

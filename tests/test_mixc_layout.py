@@ -11,7 +11,7 @@ distinct bank groups (conflicts are counted and bounded).  No GPU is used.
 import numpy as np
 import pytest
 
-SHAPES = [(7, 16, 18, 15, 288)]          # 30240
+SHAPES = [(7, 16, 18, 15, 288), (9, 14, 16, 15, 240)]          # 30240 two ways
 
 
 def w(e, L):
