@@ -210,6 +210,48 @@ const void* cfft_p2cl_kernel(int dtype, int C, int mb) {
     if (dtype == CFFT_DT_C128) return mb == 2 ? p2cl_for<double2, 2>(C) : p2cl_for<double2, 3>(C);
     return mb == 2 ? p2cl_for<float2, 2>(C) : p2cl_for<float2, 3>(C);
 }
+// both power-of-two passes in one persistent dataflow launch (pow2.cuh),
+// two CTAs per SM
+template <typename V, int N1>
+__global__ void __launch_bounds__(CFFT_THREADS, 2) k_p2flow(KParams pa, KParams pb, FlowCtl fc) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    p2flow_body<V, N1>(pa, pb, fc, smem);
+}
+template <typename V> static const void* p2flow_for(int N1) {
+    switch (N1) {
+        case 8: return (const void*)k_p2flow<V, 8>;
+        case 16: return (const void*)k_p2flow<V, 16>;
+        case 32: return (const void*)k_p2flow<V, 32>;
+        case 64: return (const void*)k_p2flow<V, 64>;
+        case 128: return (const void*)k_p2flow<V, 128>;
+        case 256: return (const void*)k_p2flow<V, 256>;
+        case 512: return (const void*)k_p2flow<V, 512>;
+        case 1024: return (const void*)k_p2flow<V, 1024>;
+    }
+    return nullptr;
+}
+const void* cfft_p2flow_kernel(int dtype, int N1) {
+    return dtype == CFFT_DT_C128 ? p2flow_for<double2>(N1) : p2flow_for<float2>(N1);
+}
+size_t cfft_p2flow_smem(size_t elem_bytes, int N1, int staged_entries) {
+    return ((16 * R4096_PL * elem_bytes + 15) & ~(size_t)15) + (129 + (size_t)N1 + staged_entries) * sizeof(double2) +
+           16;
+}
+cudaError_t cfft_launch_p2flow(const void* f, const KParams& pa, const KParams& pb, int* ctr, void* ring, int nb,
+                               int lag, int depth, unsigned grid, size_t smem, cudaStream_t st) {
+    if (!f) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(CFFT_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    KParams a = pa, b = pb;
+    FlowCtl fc = {ctr, ctr + 1, ctr + 2, ring, nb, lag, depth};
+    void* args[] = {(void*)&a, (void*)&b, (void*)&fc};
+    cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
 const void* cfft_p2row_tma_kernel(int mb) {
     return mb == 2 ? (const void*)k_p2row_tma<2> : (const void*)k_p2row_tma<3>;
 }

@@ -33,6 +33,14 @@ const void* cfft_p2col_kernel(int dtype, int N1, int mb);
 // register 4096-point CTAs, mb = 2 or 3 CTAs per SM; shared memory
 // cfft_r4096_smem
 const void* cfft_p2cl_kernel(int dtype, int C, int mb);
+// both power-of-two passes in one persistent dataflow launch (N1 = 8 ..
+// 1024): kernel, shared memory (staged_entries = w_n table entries staged,
+// or 0) and launcher; ctr (ticket, abort flag, 2 nb counters) must be zero,
+// ring holds depth intermediates of N1 x 4096 elements
+const void* cfft_p2flow_kernel(int dtype, int N1);
+size_t cfft_p2flow_smem(size_t elem_bytes, int N1, int staged_entries);
+cudaError_t cfft_launch_p2flow(const void* fn, const KParams& pa, const KParams& pb, int* ctr, void* ring, int nb,
+                               int lag, int depth, unsigned grid, size_t smem, cudaStream_t st);
 // pass A with tensor copies (ComplexF64), and its launcher (encodes the
 // tensor map of p.in for this launch)
 const void* cfft_p2row_tma_kernel(int mb);

@@ -271,7 +271,9 @@ struct Stage {
     int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
     size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
     unsigned persist = 0;    // kernels that loop over the batch: CTAs to launch at most
-    int launch = 0;          // 1: pass A by tensor copies (its own launcher)
+    int launch = 0;          // 1: pass A by tensor copies (its own launcher); 2: dataflow launch
+    KParams kp2;             // dataflow launch: the pass-B parameters
+    int flow_lag = 0, flow_depth = 0;
 };
 
 struct Shape {
@@ -330,6 +332,7 @@ struct cfft_plan_s {
     bool io_half = false;
     void* half_work = nullptr;   // batch * n ComplexF32
     void* half_dev = nullptr;    // host entry: device copy of the ComplexF16 data
+    int* flow_ctr = nullptr;     // dataflow plans: ticket, abort flag, per-transform counters (2 + 2 batch ints)
 };
 
 static size_t elem_bytes(int dtype) { return dtype == CFFT_C128 ? 16 : 8; }
@@ -511,6 +514,22 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     // 16-byte element per box row pays off once rows are 128 bytes apart;
     // measured 3-5 % faster there, 2-8 % slower at N1 = 2, 4)
     const bool tma_first = n >= 8 * 4096;
+    // both passes in one persistent dataflow launch (var = 2, N1 >= 8),
+    // offered after the two-launch forms
+    std::vector<Shape> flow;
+    if (n >= 8 * 4096) {
+        Shape s;
+        s.mode = MODE_P2COL;
+        s.conv = CONV_NONE;
+        s.M = n;
+        s.N1 = (int)(n / 4096);
+        s.N2 = 4096;
+        s.V = 2;
+        s.var = 2;
+        s.ra = radix_split(s.N1);
+        s.rc = {16, 16, 16};
+        flow.push_back(s);
+    }
     for (int c = 0; c < 4; c++) {
         const int var = ((c < 2) == tma_first) ? 1 : 0, mb = (c % 2 == 0) ? 3 : 2;
         if (dtype != CFFT_C128 && (var == 1 || mb == 2)) continue;
@@ -526,6 +545,7 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
         s.rc = {16, 16, 16};
         out.push_back(s);
     }
+    out.insert(out.end(), flow.begin(), flow.end());
     if (!cluster_first) out.insert(out.end(), cl.begin(), cl.end());
 }
 
@@ -639,7 +659,7 @@ static std::string shape_desc(const Shape& s, int64_t n) {
         return pre + "cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_P2COL)
         return "pow2(N1=" + std::to_string(s.N1) + ",N2=4096,ctas_per_sm=" + std::to_string(s.V) +
-               (s.var == 1 ? ",tma" : "") + ")";
+               (s.var == 1 ? ",tma" : s.var == 2 ? ",dataflow" : "") + ")";
     if (s.mode == MODE_FOUR)
         return pre + "four(C=" + std::to_string(s.C) + ",N1=" + std::to_string(s.N1) +
                ",N2=" + std::to_string(s.N2) + ")[" + join(s.ra) + "|" + join(s.rc) + "]";
@@ -1217,6 +1237,58 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
             put(img, v);
         }, &w1);
         if (rc) return rc;
+        if (sh.var == 2) {
+            // one persistent launch for the whole batch: a ring of `depth`
+            // intermediates (in L2 where it fits) and the item counters
+            const void* fn = cfft_p2flow_kernel(P->dtype, (int)N1);
+            if (!fn) return fail(CFFT_ERR_UNSUPPORTED, "no dataflow kernel for N1=" + std::to_string(N1));
+            const int nlo = 1 << tn.bits, nhi = (int)((n + nlo - 1) / nlo + 1);
+            const size_t base = cfft_p2flow_smem(e, (int)N1, 0), tab = (size_t)(nlo + nhi) * sizeof(double2);
+            const bool staged = base + tab <= (size_t)112 * 1024;
+            Stage st;
+            st.kp = kp;
+            st.kp.mode = MODE_P2ROW;
+            st.kp.N1 = (int)N1;
+            st.kp.N2 = 4096;
+            int lgN1 = 0;
+            while ((1LL << lgN1) < N1) lgN1++;
+            st.kp.PA = lgN1;
+            st.kp.t4 = t4096;
+            st.kp2 = kp;
+            st.kp2.mode = MODE_P2COL;
+            st.kp2.N1 = (int)N1;
+            st.kp2.N2 = 4096;
+            st.kp2.twN1 = (const double2*)w1;
+            st.kp2.t4n = tn;
+            st.kp2.pre = staged ? 1 : 0;
+            st.threads = CFFT_THREADS;
+            st.smem = cfft_p2flow_smem(e, (int)N1, staged ? nlo + nhi : 0);
+            st.cluster = 1;
+            st.in_sel = 0;
+            st.out_sel = 1;
+            st.fn = fn;
+            st.launch = 2;
+            CUDA_TRY(cfft_prepare_fn(st.fn, st.smem, 1));
+            int nsm = 0, occ = 0;
+            CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P->device));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, st.fn, CFFT_THREADS, st.smem));
+            const int resident = std::max(1, occ) * std::max(1, nsm);
+            st.persist = (unsigned)resident;
+            // a transform's tiles are claimed about twice the resident CTAs
+            // after its rows; the ring holds the transforms in between
+            st.flow_lag = (int)std::max<int64_t>(1, (resident + 2 * N1 - 1) / (2 * N1));
+            st.flow_depth = 2 * st.flow_lag + 1;
+            P->chunk = P->batch;
+            P->scratch_bytes = (size_t)st.flow_depth * n * e;
+            if (!P->shared_scratch) {
+                CUDA_TRY(lib_malloc(&P->scratch[0], P->scratch_bytes));
+                P->allocs.push_back(P->scratch[0]);
+            }
+            CUDA_TRY(lib_malloc(&P->flow_ctr, (size_t)(2 + 2 * P->batch) * sizeof(int)));
+            P->allocs.push_back(P->flow_ctr);
+            P->stages.push_back(st);
+            return CFFT_OK;
+        }
         int64_t chunk = std::max<int64_t>(1, scratch_budget(true) / (int64_t)(n * e));
         chunk = std::min<int64_t>(chunk, P->batch);
         P->chunk = chunk;
@@ -1385,6 +1457,7 @@ static void plan_free(cfft_plan_s* P) {
     P->tables.clear();
     P->stages.clear();
     P->scratch[0] = P->scratch[1] = nullptr;
+    P->flow_ctr = nullptr;
 }
 
 // in_dist / out_dist: elements between consecutive transforms of the caller's
@@ -1426,8 +1499,25 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
             else if (kp.mode == MODE_COLPASS) grid = (unsigned)(nb * (kp.N2 / kp.V));
             else grid = (unsigned)(nb * (kp.N1 / kp.V));
             if (s.persist && grid > s.persist) grid = s.persist;
-            cudaError_t ce = s.launch == 1 ? cfft_launch_p2row_tma(s.fn, kp, grid, s.smem, st)
-                                           : cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
+            cudaError_t ce;
+            if (s.launch == 2) {
+                // pass A reads the caller's input, pass B writes the caller's output
+                KParams kb = s.kp2;
+                kb.dir = kp.dir;
+                kb.scale = kp.scale;
+                kb.batch = (int)nb;
+                kb.out = kp.out;
+                kb.out_dist = odist;
+                kp.batch = (int)nb;
+                ce = cudaMemsetAsync(P->flow_ctr, 0, (size_t)(2 + 2 * nb) * sizeof(int), st);
+                if (ce == cudaSuccess)
+                    ce = cfft_launch_p2flow(s.fn, kp, kb, P->flow_ctr, P->scratch[0], (int)nb, s.flow_lag,
+                                            s.flow_depth, s.persist, s.smem, st);
+            } else if (s.launch == 1) {
+                ce = cfft_launch_p2row_tma(s.fn, kp, grid, s.smem, st);
+            } else {
+                ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
+            }
             if (ce != cudaSuccess)
                 return fail(CFFT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
         }

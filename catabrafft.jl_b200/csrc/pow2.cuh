@@ -117,7 +117,7 @@ template <int R, typename V> __device__ __forceinline__ void p2_dft_group(V* v) 
 }
 
 // stage s >= 1 of a column of N1 >= 32 (an exchange through shared memory)
-template <typename V, class PC, int s>
+template <typename V, class PC, int s, bool PF = true>
 __device__ __forceinline__ void p2col_stage(const KParams& p, V* buf, const double2* tw, int tile) {
     constexpr int r = (s < PC::A) ? 16 : PC::RL;
     constexpr int Ls = PC::N1 / p2_pow16(s);
@@ -136,7 +136,7 @@ __device__ __forceinline__ void p2col_stage(const KParams& p, V* buf, const doub
         for (int m = 0; m < r; m++) v[g * r + m] = buf[((K * Ls + tp + nb * m) << PC::LGVC) + j];
     }
     __syncthreads();                            // every read of this stage before the writes
-    if (last) {
+    if (last && PF) {
         // the buffer is free: the next tile streams in while this one finishes
         const int tn = tile + (int)gridDim.x;
         if (tn < p.batch) p2col_prefetch<V, PC>(p, buf, tn, tid);
@@ -168,11 +168,11 @@ __device__ __forceinline__ void p2col_stage(const KParams& p, V* buf, const doub
         __syncthreads();
     }
 }
-template <typename V, class PC, int s>
+template <typename V, class PC, int s, bool PF = true>
 __device__ __forceinline__ void p2col_stages(const KParams& p, V* buf, const double2* tw, int tile) {
     if constexpr (s < PC::S) {
-        p2col_stage<V, PC, s>(p, buf, tw, tile);
-        p2col_stages<V, PC, s + 1>(p, buf, tw, tile);
+        p2col_stage<V, PC, s, PF>(p, buf, tw, tile);
+        p2col_stages<V, PC, s + 1, PF>(p, buf, tw, tile);
     }
 }
 
@@ -322,4 +322,183 @@ __device__ __forceinline__ void p2cl_body(const KParams& p, unsigned char* smem)
         }
     }
     cl.sync();                                  // no CTA leaves while a peer reads its F
+}
+
+// ------------------------------------------------------------------------
+// Both passes in one persistent launch (dataflow).  Work items, claimed in
+// order from a global ticket, are the pass-A rows (N1 per transform) and the
+// pass-B column tiles (N1 per transform); slot s holds the rows of transform
+// s and the tiles of transform s - lag.  A tile of transform t waits until
+// all N1 rows of t are written; a row of transform t reuses ring slot
+// t mod depth of the intermediate and waits until all tiles of t - depth
+// have read it.  Items only wait on items claimed earlier, by CTAs that are
+// running, so the launch needs no co-residency guarantee.  Producers publish
+// with a fence and an atomic add after a block barrier; consumers acquire
+// the counter, then a block barrier.  Every wait is bounded (about a second):
+// on a timeout the item is skipped and the device fault word records it.
+struct FlowCtl {
+    int* ticket;                  // next item
+    int* abort;                   // set by the first wait that times out: later waits give up at once
+    int* cnt;                     // rows done per transform [nb], then tiles done [nb]
+    void* ring;                   // depth intermediates of n elements
+    int nb, lag, depth;           // transforms, slots between a row and its tiles, ring size
+};
+constexpr unsigned kFaultFlowTimeout = 2u;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// thread 0 waits until *c >= target (bounded, about a second); the CTA
+// learns the outcome.  The first wait of a launch that times out raises the
+// launch's abort flag, so no later wait of that launch waits at all.
+__device__ __forceinline__ bool flow_wait(const int* c, int target, int* flag, int* abort) {
+    if (threadIdx.x == 0) {
+        int ok = 0;
+        for (int it = 0; it < (1 << 23); it++) {
+            if (ld_acquire_gpu(c) >= target) { ok = 1; break; }
+            if (ld_acquire_gpu(abort)) break;
+            __nanosleep(128);
+        }
+        *flag = ok;
+        if (!ok) {
+            atomicExch(abort, 1);
+            record_fault(kFaultFlowTimeout);
+        }
+    }
+    __syncthreads();
+    const bool ok = *flag != 0;
+    __syncthreads();                            // the flag may be rewritten next
+    return ok;
+}
+// every thread's stores of this item precede the count
+__device__ __forceinline__ void flow_publish(int* c) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(c, 1);
+}
+
+// pa: pass A (in = the transforms at in_dist, PA = log2 N1, t4 = w_4096);
+// pb: pass B (out = the output at out_dist, twN1, t4n staged when pre).
+// Shared memory: 16 planes of R4096_PL elements (pass B uses the first 4096
+// slots), the w_4096 table, the w_N1 table, the staged w_n table, two ints.
+template <typename V, int N1>
+__device__ __forceinline__ void p2flow_body(const KParams& pa, const KParams& pb, const FlowCtl& fc,
+                                            unsigned char* smem) {
+    using PC = P2Col<N1>;
+    V* buf = (V*)smem;
+    double2* tlo = after16(buf + 16 * R4096_PL);
+    double2* thi = tlo + 64;
+    double2* tw = thi + 65;                     // w_N1, N1 entries
+    double2* ts = tw + N1;                      // staged w_n two-level table
+    const int bits = pb.t4n.bits;
+    const int nlo = 1 << bits, nhi = (pb.t4n.N + nlo - 1) / nlo + 1;
+    int* sh = (int*)(ts + (pb.pre ? nlo + nhi : 0));
+    const double2 *lo = pb.t4n.lo, *hi = pb.t4n.hi;
+    {
+        const int t = opaque_tid();
+        if (t < 64) tlo[t ^ (t >> 3)] = pa.t4.lo[t];
+        if (t < 65) thi[t] = pa.t4.hi[t];
+        for (int i = t; i < N1; i += 256) tw[i] = pb.twN1[i];
+        if (pb.pre) {
+            for (int i = t; i < nlo + nhi; i += 256) ts[i] = (i < nlo) ? pb.t4n.lo[i] : pb.t4n.hi[i - nlo];
+            lo = ts;
+            hi = ts + nlo;
+        }
+    }
+    const long long n = (long long)N1 * 4096;
+    const int per = 2 * N1;
+    const long long total = (long long)(fc.nb + fc.lag) * per;
+    for (;;) {
+        if (threadIdx.x == 0) sh[0] = atomicAdd(fc.ticket, 1);
+        __syncthreads();                        // also: tables staged, buffer free
+        const long long w = sh[0];
+        __syncthreads();
+        if (w >= total) break;
+        const int s = (int)(w / per), r = (int)(w - (long long)s * per);
+        if (r < N1) {
+            // ---- pass A: row i of transform s
+            const int tr = s, i = r;
+            if (tr >= fc.nb) continue;
+            if (tr >= fc.depth && !flow_wait(fc.cnt + fc.nb + (tr - fc.depth), N1, sh + 1, fc.abort)) continue;
+            V v[16];
+            {
+                const int t = opaque_tid();
+                const V* in = (const V*)pa.in + (long long)tr * pa.in_dist + i + (t << PC::LGN1);
+#pragma unroll 1
+                for (int k = 0; k < 16; k++, in += 256LL << PC::LGN1) cp_async_elem(buf + t + 256 * k, in);
+                cp_async_commit();
+                cp_async_wait_all();            // this thread's own slots
+#pragma unroll
+                for (int k = 0; k < 16; k++) v[k] = load_in(pa, buf[t + 256 * k]);
+            }
+            fft4096_regs(v, buf, tlo, thi, opaque_tid());
+            {
+                const int t = opaque_tid();
+                V* row = (V*)fc.ring + (long long)(tr % fc.depth) * n + ((long long)i << 12);
+#pragma unroll
+                for (int k3 = 0; k3 < 16; k3++) row[t + 256 * k3] = v[k3];
+            }
+            flow_publish(fc.cnt + tr);
+        } else {
+            // ---- pass B: column tile of transform s - lag
+            const int tr = s - fc.lag, tile_in_tr = r - N1;
+            if (tr < 0 || tr >= fc.nb) continue;
+            if (!flow_wait(fc.cnt + tr, N1, sh + 1, fc.abort)) continue;
+            // the tile's view of the intermediate as a pass-B launch of one transform
+            KParams q = pb;
+            q.in = (const V*)fc.ring + (long long)(tr % fc.depth) * n;
+            q.in_dist = n;
+            q.out = (V*)pb.out + (long long)tr * pb.out_dist;
+            const int tid = opaque_tid();
+            p2col_prefetch<V, PC>(q, buf, tile_in_tr, tid);
+            cp_async_commit();
+            cp_async_wait_all();
+            V v[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) v[k] = buf[tid + 256 * k];
+            const int c0 = tile_in_tr * PC::VC;
+            V* out = (V*)q.out;
+            if constexpr (N1 <= 16) {
+                __syncwarp();
+                p2col_discard<V, PC>(q, tile_in_tr, tid);
+#pragma unroll
+                for (int g = 0; g < PC::CPT; g++) {
+                    V u[N1];
+                    const unsigned col = (unsigned)(c0 + tid + 256 * g);
+                    const double2 st = p2_wn(lo, hi, bits, col);
+                    double2 wv = st;
+                    u[0] = v[g];
+#pragma unroll
+                    for (int m = 1; m < N1; m++) {
+                        u[m] = cmul(v[g + PC::CPT * m], fromd<V>(wv));
+                        if (m + 1 < N1) wv = cmul(wv, st);
+                    }
+                    dft<N1>(u);
+#pragma unroll
+                    for (int k = 0; k < N1; k++) p2col_store(q, out, (int)col, k, u[k]);
+                }
+            } else {
+                const int j = tid & (PC::VC - 1), b = tid >> PC::LGVC;
+                {
+                    const unsigned col = (unsigned)(c0 + j);
+                    double2 wv = p2_wn(lo, hi, bits, col * (unsigned)b);
+                    const double2 st = p2_wn(lo, hi, bits, col * (unsigned)PC::TPC);
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        v[k] = cmul(v[k], fromd<V>(wv));
+                        if (k < 15) wv = cmul(wv, st);
+                    }
+                }
+                dft<16>(v);
+#pragma unroll
+                for (int k = 0; k < 16; k++) buf[tid + 256 * k] = p2_tw_stage(v[k], tw, (unsigned)(b * k));
+                __syncthreads();
+                p2col_discard<V, PC>(q, tile_in_tr, tid);
+                p2col_stages<V, PC, 1, false>(q, buf, tw, tile_in_tr);
+            }
+            flow_publish(fc.cnt + fc.nb + tr);
+        }
+    }
 }

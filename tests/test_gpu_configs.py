@@ -279,3 +279,31 @@ def test_pow2_cluster_three_ctas_per_sm(cb, tmp_path):
                             flags=cb.MEASURE)
         finally:
             cb.forget_wisdom()
+
+
+def test_pow2_dataflow_single_launch(cb, tmp_path):
+    """Both power-of-two passes in one persistent dataflow launch (rows and
+    column tiles claimed from a ticket, per-transform counters, a ring of
+    intermediates), reached through wisdom entries for MEASURE plans: one
+    launch per execution, every variant's parity, no timed-out wait."""
+    cases = [(1 << 15, 600), (1 << 16, 300), (1 << 18, 40), (1 << 20, 9), (1 << 22, 5)]
+    cb._lib.LIB.cfft_device_faults(1)
+    for dtype, code in ((np.complex128, 0), (np.complex64, 1)):
+        lines = ["catabra-b200-wisdom 1"]
+        for n, batch in cases:
+            N1 = n // 4096
+            sig = f"4 0 {n} {N1} 4096 1 2 a {' '.join(map(str, _greedy_split(N1)))} c 16 16 16 v2"
+            lines.append(f"{n} {batch} {code} {cb.MEASURE} | {sig}")
+        path = tmp_path / f"f{code}.txt"
+        path.write_text("\n".join(lines) + "\n")
+        cb.forget_wisdom()
+        cb.import_wisdom(str(path))
+        try:
+            for n, batch in cases:
+                with _CPlan(cb, n, batch, cb.C128 if code == 0 else cb.C64, cb.MEASURE) as p:
+                    assert p.launches() == 1, (n, p.describe())
+                _pow2_check(cb, n, batch, dtype, f"pow2(N1={n // 4096},N2=4096,ctas_per_sm=2,dataflow)",
+                            flags=cb.MEASURE)
+        finally:
+            cb.forget_wisdom()
+    assert cb._lib.LIB.cfft_device_faults(1) == 0
