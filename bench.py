@@ -329,6 +329,8 @@ def form_precision(torch, cb, lib, dev, args):
     4096 x 3^9, uniform(-1,1) parts; error vs this library's ComplexF64 path
     (itself held to 1e-12 of the oracle by the tests)."""
     sizes = [(65536, args.batch or 4096), (19683, args.batch or 4096)]
+    if args.only:
+        sizes = [(n, b) for n, b in sizes if n == args.only]
     g = torch.Generator(device=dev)
     g.manual_seed(11)
     st = torch.cuda.current_stream(dev)

@@ -32,6 +32,7 @@
 
 #include "../../include/catabra_b200.h"
 #include "kernels.h"
+#include "trace.h"
 
 // thread-local error text in a fixed buffer (set without touching the heap)
 static thread_local char g_err[512];
@@ -2109,6 +2110,7 @@ static void serve_finish(cfft_server_s* S, const std::vector<int64_t>& reqs, int
 
 // one micro-batch on an idle slot: grouped launches, then the slot's event
 static int serve_launch(cfft_server_s* S, ServeSlot& sl) {
+    cfft_trace::Range tr("serve_batch requests=%lld", (long long)sl.reqs.size(), 0);
     struct It { KParams kp; double cost; size_t smem; };
     std::map<std::tuple<const void*, int, int>, std::vector<It>> singles;
     std::map<std::tuple<const void*, int>, std::vector<It>> pass[4];
@@ -2422,6 +2424,7 @@ int64_t cfft_debug_alloc_hook(int64_t nth) {
 }
 
 int cfft_plan_create(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags) {
+    cfft_trace::Range tr("plan_create n=%lld batch=%lld dtype=%lld flags=%lld", n, batch, dtype, flags);
     g_err[0] = 0;
     return plan_create_impl(plan, n, batch, dtype, flags);
 }
@@ -2452,6 +2455,7 @@ static int execute_strided(cfft_plan_s* P, const void* d_in, void* d_out, int di
 
 int cfft_plan_create_many(cfft_plan* plan, int64_t n, int64_t batch, int dtype, int flags, int64_t istride,
                           int64_t idist, int64_t ostride, int64_t odist) {
+    cfft_trace::Range tr("plan_create_many n=%lld batch=%lld istride=%lld ostride=%lld", n, batch, istride, ostride);
     g_err[0] = 0;
     if (!plan) return fail(CFFT_ERR_INVALID, "plan pointer is null");
     if (istride < 1 || ostride < 1 || idist < 0 || odist < 0)
@@ -2480,6 +2484,7 @@ int cfft_plan_create_many(cfft_plan* plan, int64_t n, int64_t batch, int dtype, 
 }
 
 int cfft_execute(cfft_plan plan, const void* d_in, void* d_out, int direction, void* stream) {
+    cfft_trace::Range tr(plan ? plan->desc.c_str() : "execute");
     if (!plan || !d_in || !d_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (plan->io_half) return execute_half(plan, d_in, d_out, direction, (cudaStream_t)stream);
     if (plan->strided) return execute_strided(plan, d_in, d_out, direction, (cudaStream_t)stream);
@@ -2564,6 +2569,7 @@ static int execute_host_staged(cfft_plan_s* P, const void* h_in, void* h_out, in
 }
 
 int cfft_execute_host(cfft_plan plan, const void* h_in, void* h_out, int direction) {
+    cfft_trace::Range tr("execute_host n=%lld batch=%lld", plan ? plan->n : 0, plan ? plan->batch : 0);
     if (!plan || !h_in || !h_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
     cfft_plan_s* P = plan;
@@ -2640,6 +2646,7 @@ int cfft_plan_destroy(cfft_plan plan) {
 
 int cfft_fft(int64_t n, int64_t batch, int dtype, int flags, const void* d_in, void* d_out,
              int direction, void* stream) {
+    cfft_trace::Range tr("fft n=%lld batch=%lld dtype=%lld flags=%lld", n, batch, dtype, flags);
     int dev = 0;
     cudaGetDevice(&dev);
     cfft_plan_s* P = nullptr;
@@ -2659,6 +2666,7 @@ int cfft_fft(int64_t n, int64_t batch, int dtype, int flags, const void* d_in, v
 }
 
 int cfft_empty_cache(void) {
+    cfft_trace::Range tr("empty_cache");
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
         for (auto& kv : g_cache) {
@@ -2701,6 +2709,7 @@ int64_t cfft_plan_workspace_bytes(cfft_plan plan) {
 
 
 int cfft_batch_create(cfft_batch* batch, int64_t count, const int64_t* lengths, int dtype, int flags) {
+    cfft_trace::Range tr("batch_create count=%lld dtype=%lld", count, dtype);
     g_err[0] = 0;
     if (!batch || !lengths || count < 1) return fail(CFFT_ERR_INVALID, "batch, lengths and count >= 1 required");
     if (dtype != CFFT_C128 && dtype != CFFT_C64) return fail(CFFT_ERR_INVALID, "dtype must be CFFT_C128 or CFFT_C64");
@@ -2718,6 +2727,7 @@ int cfft_batch_create(cfft_batch* batch, int64_t count, const int64_t* lengths, 
 }
 
 int cfft_batch_execute(cfft_batch batch, const void* d_in, void* d_out, int direction, void* stream) {
+    cfft_trace::Range tr("batch_execute count=%lld dir=%lld", batch ? batch->count : 0, direction);
     if (!batch || !d_in || !d_out) return fail(CFFT_ERR_INVALID, "null batch or buffer");
     if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
     cfft_batch_s* B = batch;
@@ -2775,6 +2785,7 @@ int cfft_plan_launches(cfft_plan plan) {
 
 int cfft_serve_create(cfft_server* server, int dtype, int64_t max_inflight_bytes, int64_t max_requests,
                       int mode) {
+    cfft_trace::Range tr("serve_create dtype=%lld cap=%lld", dtype, max_inflight_bytes);
     g_err[0] = 0;
     if (!server) return fail(CFFT_ERR_INVALID, "server pointer is null");
     *server = nullptr;
@@ -2930,6 +2941,7 @@ int cfft_serve_destroy(cfft_server server) {
 // Wisdom file: a header line, then one line per entry:
 //   n batch dtype flags | mode conv M N1 N2 C V a <radices> c <radices>
 int cfft_wisdom_export(const char* path) {
+    cfft_trace::Range tr("wisdom_export");
     if (!path) return fail(CFFT_ERR_INVALID, "null path");
     FILE* f = fopen(path, "w");
     if (!f) return fail(CFFT_ERR_INVALID, std::string("cannot write ") + path);
@@ -2944,6 +2956,7 @@ int cfft_wisdom_export(const char* path) {
 }
 
 int cfft_wisdom_import(const char* path) {
+    cfft_trace::Range tr("wisdom_import");
     if (!path) return fail(CFFT_ERR_INVALID, "null path");
     FILE* f = fopen(path, "r");
     if (!f) return fail(CFFT_ERR_INVALID, std::string("cannot read ") + path);
@@ -3001,6 +3014,7 @@ struct cfft_rplan_s {
 };
 
 int cfft_rfft_plan_create(cfft_rplan* plan, int64_t n, int64_t batch, int dtype, int flags) {
+    cfft_trace::Range tr("rfft_plan_create n=%lld batch=%lld dtype=%lld flags=%lld", n, batch, dtype, flags);
     g_err[0] = 0;
     if (!plan) return fail(CFFT_ERR_INVALID, "plan pointer is null");
     *plan = nullptr;
@@ -3033,6 +3047,7 @@ int cfft_rfft_plan_create(cfft_rplan* plan, int64_t n, int64_t batch, int dtype,
 }
 
 int cfft_rfft_execute(cfft_rplan plan, const void* d_real, void* d_complex, void* stream) {
+    cfft_trace::Range tr("rfft_execute");
     if (!plan || !d_real || !d_complex) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     cfft_rplan_s* R = plan;
     const size_t e = elem_bytes(R->dtype);
@@ -3054,6 +3069,7 @@ int cfft_rfft_execute(cfft_rplan plan, const void* d_real, void* d_complex, void
 }
 
 int cfft_rfft_execute_inverse(cfft_rplan plan, const void* d_complex, void* d_real, int direction, void* stream) {
+    cfft_trace::Range tr("rfft_execute_inverse");
     if (!plan || !d_real || !d_complex) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (direction != CFFT_INVERSE && direction != CFFT_BACKWARD)
         return fail(CFFT_ERR_INVALID, "direction must be CFFT_INVERSE (irfft) or CFFT_BACKWARD (brfft)");
@@ -3076,6 +3092,7 @@ int cfft_rfft_execute_inverse(cfft_rplan plan, const void* d_complex, void* d_re
 }
 
 int cfft_rfft_execute_host(cfft_rplan plan, const void* h_in, void* h_out, int direction) {
+    cfft_trace::Range tr("rfft_execute_host");
     if (!plan || !h_in || !h_out) return fail(CFFT_ERR_INVALID, "null plan or buffer");
     if (direction < 0 || direction > 2) return fail(CFFT_ERR_INVALID, "direction must be 0, 1 or 2");
     cfft_rplan_s* R = plan;
