@@ -465,21 +465,16 @@ def form_pow2(torch, cb, lib, dev, args):
 
 def form_batch(torch, cb, lib, dev, args):
     """20000 mixed lengths in [16, 2^20] (half 7-smooth, half with a prime
-    factor <= 65537), one graph launch per execution; against the same
-    transforms as per-request plan executions."""
+    factor <= 65537), one graph launch (one work-queue kernel) per
+    execution; against the grouped schedule and against the same transforms
+    as per-request plan executions."""
     import importlib
     w = importlib.import_module("catabra_b200.workloads")
     lengths = [int(v) for v in w.batch_lengths(args.count, seed=1)]
     st = torch.cuda.current_stream(dev)
     res = {}
-    for name, dt, tdt, e in (("c64", np.complex64, torch.complex64, 8),
-                             ("c128", np.complex128, torch.complex128, 16)):
-        t0 = time.perf_counter()
-        b = cb.Batch(lengths, dt)
-        t_plan = time.perf_counter() - t0
-        x = torch.randn(b.total, dtype=tdt, device=dev)
-        y = torch.empty_like(x)
-        for _ in range(args.warmup):
+    def timed(b, x, y):
+        for _ in range(max(3, args.warmup)):
             b.execute(x, out=y)
         steps = max(3, min(args.steps, 10))
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -489,7 +484,23 @@ def form_batch(torch, cb, lib, dev, args):
             b.execute(x, out=y)
         z.record(st)
         torch.cuda.synchronize()
-        ms = a.elapsed_time(z) / steps
+        return a.elapsed_time(z) / steps
+
+    for name, dt, tdt, e in (("c64", np.complex64, torch.complex64, 8),
+                             ("c128", np.complex128, torch.complex128, 16)):
+        t0 = time.perf_counter()
+        b = cb.Batch(lengths, dt)
+        t_plan = time.perf_counter() - t0
+        x = torch.randn(b.total, dtype=tdt, device=dev)
+        y = torch.empty_like(x)
+        ms = timed(b, x, y)
+        assert lib.cfft_device_faults(1) == 0
+        # the grouped schedule on the same stream (context)
+        bg = cb.Batch(lengths, dt, cb.BATCH_GROUPED)
+        ms_g = timed(bg, x, torch.empty_like(x))
+        launches_g = bg.launches()
+        bg.close()
+        torch.cuda.empty_cache()
         # per-request path: every transform launched on its own through its
         # cached plan (the serving engine's direct mode: one plan per length,
         # one shared two-pass scratch), host-timed from the first launch to
@@ -512,11 +523,12 @@ def form_batch(torch, cb, lib, dev, args):
                      "per_request_ms": round(ms_req, 3),
                      "per_request_GB_s": round(nbytes / (ms_req * 1e-3) / 1e9, 2),
                      "speedup_vs_per_request": round(ms_req / ms, 2), "launches": b.launches(),
+                     "grouped_ms_per_batch": round(ms_g, 3), "grouped_launches": launches_g,
                      "plan_s": round(t_plan, 2), "elements": b.total}
         b.close()
         del x, y
         torch.cuda.empty_cache()
-    return {"form": "batch", "metric": "FFT GB/s, one graph launch over mixed lengths",
+    return {"form": "batch", "metric": "FFT GB/s, one queue launch over mixed lengths",
             "value": res["c64"]["GB_s"], "unit": "GB/s", "higher_is_better": True, "per_dtype": res,
             "config": {"workload": f"{args.count} lengths log-uniform in [16, 2^20], half 7-smooth, "
                                    "half with a prime factor <= 65537 (seed 1), forward"}}

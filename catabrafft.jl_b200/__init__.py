@@ -28,7 +28,7 @@ import threading
 import numpy as np
 
 from . import _lib
-from ._lib import (BACKWARD, C32, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERSE, MEASURE,
+from ._lib import (BACKWARD, BATCH_GROUPED, C32, C64, C128, ENCHANT, EXACT_TWIDDLES, FORWARD, INVERSE, MEASURE,
                    NO_FLAG, SERVE_BATCHED, SERVE_DIRECT, CatabraError, check)
 
 FLAG = int
@@ -38,7 +38,7 @@ __all__ = ["fft", "ifft", "bfft", "fft_", "plan_fft", "Spell", "mul_", "empty_ca
            "export_wisdom", "import_wisdom", "forget_wisdom", "wisdom_entries",
            "rfft", "irfft", "brfft", "plan_rfft", "plan_brfft", "RSpell", "plan_bfft", "plan_ifft",
            "plan_inv", "fftn", "ifftn", "fft2", "ifft2",
-           "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "FLAG", "CatabraError",
+           "NO_FLAG", "MEASURE", "ENCHANT", "EXACT_TWIDDLES", "BATCH_GROUPED", "FLAG", "CatabraError",
            "describe_strategy", "version"]
 
 _cache_lock = threading.Lock()

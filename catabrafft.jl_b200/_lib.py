@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libcatabra_b200.so")
 
 C128, C64, C32 = 0, 1, 2
 FORWARD, INVERSE, BACKWARD = 0, 1, 2
-NO_FLAG, MEASURE, ENCHANT, EXACT_TWIDDLES = 0, 1, 2, 16
+NO_FLAG, MEASURE, ENCHANT, EXACT_TWIDDLES, BATCH_GROUPED = 0, 1, 2, 16, 32
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED = 0, 1, 2, 3, 4
 SERVE_BATCHED, SERVE_DIRECT = 0, 1
 

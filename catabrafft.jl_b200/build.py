@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libcatabra_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 
-DEVICE_SOURCES = ["kernels.cu", "noalloc.cu", "tables.cu", "real.cu"]
+DEVICE_SOURCES = ["kernels.cu", "queue.cu", "noalloc.cu", "tables.cu", "real.cu"]
 HOST_SOURCES = ["plan.cpp"]
 
 

@@ -134,3 +134,28 @@ struct BatchLaunch {
     int pad_;
 };
 
+
+// The batched form's single persistent launch: CTAs claim work items in
+// ticket order; an item is one block of a parameter block (a whole
+// single-CTA transform, or one tile of a two-pass stage).  An item may wait
+// for a counter to reach `need` (the previous stage of its transform, or the
+// release of the scratch half its chunk reuses) and adds one to counter
+// `done` when finished.  Every wait is on items with smaller tickets, so the
+// queue drains whatever the residency.
+enum { QK_ROWS = 0, QK_FOUR = 1, QK_FOUR_WARP = 2, QK_COLPASS = 3, QK_ROWPASS = 4 };
+struct QItem {
+    int desc;                     // parameter block
+    int blk;                      // block within the parameter block
+    int kind;                     // QK_*
+    int wait, need;               // counter (-1: none) and the count to wait for
+    int done;                     // counter to add one to (-1: none)
+};
+struct QueueLaunch {
+    const KParams* desc;
+    const QItem* items;
+    const void* in_base;
+    void* out_base;
+    int* ctl;                     // [0] ticket, [1] abort flag, [2 ...] counters; zero before each launch
+    int nitems;
+    int dir;                      // direction of every item, or -1: each parameter block's own
+};

@@ -312,12 +312,17 @@ cudaError_t cfft_wait_probe(int polls) {
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return e;
 }
+// each translation unit with kernels that record faults has its own copy of
+// the word: this one's, OR-ed with the queue kernel's (queue.cu)
 cudaError_t cfft_device_fault_word(unsigned* out, int clear) {
     cudaError_t e = cudaMemcpyFromSymbol(out, g_cfft_fault, sizeof(unsigned));
     if (e == cudaSuccess && clear) {
         const unsigned z = 0;
         e = cudaMemcpyToSymbol(g_cfft_fault, &z, sizeof(unsigned));
     }
+    unsigned q = 0;
+    if (e == cudaSuccess) e = cfft_queue_fault_word(&q, clear);
+    if (e == cudaSuccess) *out |= q;
     return e;
 }
 const void* cfft_p2row_kernel(int dtype, int mb) {

@@ -71,6 +71,12 @@ cudaError_t cfft_max_active_clusters_fn(const void* fn, int threads, size_t smem
 const void* cfft_batch_kernel_for(int mode, int dtype);
 cudaError_t cfft_launch_batch(const void* fn, const BatchLaunch& L, unsigned grid, size_t smem,
                               int cluster, cudaStream_t stream);
+// the batched form's persistent queue kernel (QueueLaunch, queue.cu), built
+// for mb = 2 or 3 CTAs per SM, its launcher (ctl must be zero) and its
+// translation unit's copy of the device fault word
+const void* cfft_queue_kernel(int dtype, int mb);
+cudaError_t cfft_launch_queue(const void* fn, const QueueLaunch& L, unsigned grid, size_t smem, cudaStream_t st);
+cudaError_t cfft_queue_fault_word(unsigned* out, int clear);
 // convolution tables on the device (tables.cu)
 cudaError_t cfft_gen_chirp(double2* ch, long long n, cudaStream_t st);
 cudaError_t cfft_gen_bluestein_b(double2* b, const double2* ch, long long n, long long M, cudaStream_t st);

@@ -600,6 +600,25 @@ static void mixc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     }
 }
 
+// two HBM passes (COLPASS then ROWPASS; a convolution runs two of each);
+// Rader here becomes Bluestein, and a convolution may use any 7-smooth
+// length >= its minimum: take the first that splits into two factors of at
+// most 4096
+static bool twopass_shape(int64_t n, int conv, int64_t M, int dtype, Shape& g) {
+    int c2 = conv;
+    int64_t M2 = M;
+    if (conv == CONV_RADER) { c2 = CONV_BLUE; M2 = smooth_ceil(2 * n - 1); }
+    for (int tries = 0; tries < 256; tries++) {
+        if (global_shape(M2, dtype, g)) {
+            g.conv = c2;
+            return true;
+        }
+        if (c2 == CONV_NONE) return false;
+        M2 = smooth_ceil(M2 + 1);
+    }
+    return false;
+}
+
 static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) {
     std::vector<Shape> v;
     int conv;
@@ -611,31 +630,17 @@ static std::vector<Shape> candidate_shapes(int64_t n, int dtype, int64_t batch) 
         v.push_back(sh);
     }
     if (M > 64) four_candidates(M, n, conv, dtype, v);
-    if (v.empty() || M >= 16384) {
-        // beyond a cluster (or as the timed planners' alternative to one):
-        // two HBM passes; Rader here becomes Bluestein
-        int c2 = conv;
-        int64_t M2 = M;
-        if (conv == CONV_RADER) { c2 = CONV_BLUE; M2 = smooth_ceil(2 * n - 1); }
-        // a convolution may use any 7-smooth length >= its minimum: take the
-        // first that splits into two factors of at most 4096
-        Shape g;
-        for (int tries = 0; tries < 256; tries++) {
-            if (global_shape(M2, dtype, g)) {
-                g.conv = c2;
-                // measured on B200: from 2^15 points the two passes beat a
-                // cluster for ComplexF32 transforms (1.3-1.5x at 2^16-2^17)
-                // and for power-of-two ComplexF64 ones (1.3x at 2^15, 1.7x
-                // at 2^16); otherwise second in line, so the heuristic keeps
-                // a single-kernel shape and MEASURE/ENCHANT time both
-                const bool pow2 = (M & (M - 1)) == 0;
-                const bool first = (dtype == CFFT_C64 || pow2) && conv == CONV_NONE && M >= 32768;
-                v.insert(v.begin() + (first ? 0 : std::min<size_t>(v.size(), 1)), g);
-                break;
-            }
-            if (c2 == CONV_NONE) break;
-            M2 = smooth_ceil(M2 + 1);
-        }
+    Shape g;
+    if ((v.empty() || M >= 16384) && twopass_shape(n, conv, M, dtype, g)) {
+        // beyond a cluster (or as the timed planners' alternative to one).
+        // Measured on B200: from 2^15 points the two passes beat a cluster
+        // for ComplexF32 transforms (1.3-1.5x at 2^16-2^17) and for
+        // power-of-two ComplexF64 ones (1.3x at 2^15, 1.7x at 2^16);
+        // otherwise second in line, so the heuristic keeps a single-kernel
+        // shape and MEASURE/ENCHANT time both
+        const bool pow2 = (M & (M - 1)) == 0;
+        const bool first = (dtype == CFFT_C64 || pow2) && conv == CONV_NONE && M >= 32768;
+        v.insert(v.begin() + (first ? 0 : std::min<size_t>(v.size(), 1)), g);
     }
     // the register kernels lead for the lengths they cover
     std::vector<Shape> reg;
@@ -1703,15 +1708,23 @@ static int plan_create_impl(cfft_plan_s** out, int64_t n, int64_t batch, int dty
 
 
 // ------------------------------------------------------------ batched form
-// Many transforms of mixed lengths packed back to back.  Every transform gets
-// a parameter block in device memory; transforms whose plan is a single
-// kernel (rows or cluster four-step) are grouped by kernel variant, cluster
-// size and shared-memory class, and each group runs as one launch whose
-// blocks look up their parameter block.  Transforms that need two HBM passes
-// run through their plan's launches on a scratch shared by the whole batch.
-// Groups are ordered largest transform first (longest-processing-time
-// order) so the block scheduler balances the tail.  The whole sequence is
-// captured once into a CUDA graph per (input, output, direction).
+// Many transforms of mixed lengths packed back to back, captured once into a
+// CUDA graph per (input, output, direction).  Two schedules:
+//  * work queue (default): every transform is planned as a single-CTA
+//    kernel (rows, or a one-CTA four-step) that fits the queue kernel's
+//    shared-memory budget, or else as two HBM passes; the work items (whole
+//    single-CTA transforms and pass tiles) run in one launch whose CTAs each
+//    claim the next item by ticket (kq_batch, QItem): two-pass transforms
+//    largest first in chunks that
+//    take turns on a ring of scratch slots (a chunk's first pass waits for
+//    the chunk that last used its slot to finish), each stage's tiles waiting for
+//    the previous stage of their transform, then the single-CTA transforms
+//    largest first to fill the tail;
+//  * grouped (CFFT_BATCH_GROUPED): transforms whose plan is a single kernel
+//    (rows or cluster four-step) are grouped by kernel variant, cluster size
+//    and shared-memory class, each group one launch whose blocks look up
+//    their parameter block; two-pass transforms run pass by pass on a shared
+//    scratch; groups largest first (longest-processing-time order).
 struct cfft_batch_s {
     int dtype = 0, flags = 0, device = 0;
     int64_t count = 0, total = 0;
@@ -1727,8 +1740,17 @@ struct cfft_batch_s {
         int ndesc = 0;
         double cost = 0;
     };
-    std::vector<Group> groups;   // single-kernel transforms
-    std::vector<Group> passes;   // two-pass transforms, chunk by chunk, pass by pass
+    std::vector<Group> groups;   // grouped form: single-kernel transforms
+    std::vector<Group> passes;   // grouped form: two-pass transforms, chunk by chunk, pass by pass
+    // queue form (the default): one launch over every work item
+    bool queue = false;
+    const void* qfn = nullptr;
+    KParams* q_desc = nullptr;
+    QItem* q_items = nullptr;
+    int* q_ctl = nullptr;
+    int q_nitems = 0, q_nctl = 0;
+    unsigned q_grid = 0;
+    size_t q_smem = 0;
     void* scratch[2] = {nullptr, nullptr};
     std::vector<void*> allocs;
     cudaStream_t cap = nullptr;
@@ -1772,6 +1794,52 @@ static int build_shared_plan(int64_t n, int dtype, int flags, int device, cfft_p
         if (c.mode == MODE_P2COL || c.mode == MODE_CONVC || c.mode == MODE_MIXC || c.mode == MODE_P2CL) continue;
         rc = plan_build(P, c);
         if (rc == CFFT_OK) break;
+        plan_free(P);
+    }
+    if (rc) {
+        delete P;
+        return rc;
+    }
+    *out = P;
+    return CFFT_OK;
+}
+// batch-1 plan for the work queue: a single-CTA shape (rows or a
+// one-CTA four-step) whose descriptor-driven variant fits `cap` bytes of
+// shared memory, else two HBM passes
+static size_t batched_smem(const Stage& st);
+static bool single_kernel(const cfft_plan_s* P);
+static int build_queue_plan(int64_t n, int dtype, int flags, int device, size_t cap, cfft_plan_s** out) {
+    if (n > (1LL << 26)) return fail(CFFT_ERR_UNSUPPORTED, "length above 2^26");
+    std::vector<Shape> v;
+    for (auto& c : candidate_shapes(n, dtype, 1))
+        if ((c.mode == MODE_ROWS || c.mode == MODE_FOUR) && c.C == 1) v.push_back(c);
+    int conv;
+    int64_t M;
+    conv_kind(n, conv, M);
+    Shape g;
+    if (twopass_shape(n, conv, M, dtype, g)) v.push_back(g);
+    cfft_plan_s* P = new cfft_plan_s();
+    P->n = n;
+    P->batch = 1;
+    P->dtype = dtype;
+    P->flags = flags;
+    P->device = device;
+    P->shared_scratch = true;
+    int rc = fail(CFFT_ERR_UNSUPPORTED, "no queue shape for n=" + std::to_string(n));
+    for (auto& c : v) {
+        rc = plan_build(P, c);
+        if (rc == CFFT_OK) {
+            bool ok = true;
+            if (single_kernel(P)) {
+                ok = P->stages[0].cluster <= 1 && batched_smem(P->stages[0]) <= cap;
+            } else {
+                for (auto& st : P->stages)
+                    ok = ok && (st.kp.mode == MODE_COLPASS || st.kp.mode == MODE_ROWPASS) && st.smem <= cap;
+            }
+            if (ok) break;
+            rc = fail(CFFT_ERR_UNSUPPORTED, "no queue shape within the shared-memory budget for n=" +
+                                                std::to_string(n));
+        }
         plan_free(P);
     }
     if (rc) {
@@ -1842,6 +1910,205 @@ static int make_group(cfft_batch_s* B, const void* fn, int cluster, std::vector<
     return CFFT_OK;
 }
 
+// work-queue schedule (see the batched form's header): plans,
+// parameter blocks, work items and counters, uploaded once
+static int batch_create_queue(cfft_batch_s* B) {
+    const int dtype = B->dtype;
+    const size_t e = elem_bytes(dtype);
+    const int dt = dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64;
+    // ComplexF64 at two CTAs per SM, ComplexF32 at three (the pass kernels'
+    // residency); the shared-memory budget per CTA follows
+    const int mb = dtype == CFFT_C128 ? 2 : 3;
+    const size_t cap = mb == 3 ? (size_t)74 * 1024 : (size_t)112 * 1024;
+    for (int64_t n : B->len) {
+        if (B->plans.count(n)) continue;
+        cfft_plan_s* P = nullptr;
+        int rc = build_queue_plan(n, dtype, B->flags, B->device, cap, &P);
+        if (rc) return rc;
+        B->plans[n] = P;
+    }
+    std::vector<KParams> desc;
+    std::vector<QItem> items;
+    int nctr = 0;
+    size_t smax = 0;
+    std::vector<int64_t> twopass, singles;
+    for (int64_t i = 0; i < B->count; i++) (single_kernel(B->plans[B->len[i]]) ? singles : twopass).push_back(i);
+    auto by_len = [&](int64_t a, int64_t b) { return B->len[a] > B->len[b]; };
+    std::stable_sort(twopass.begin(), twopass.end(), by_len);
+    std::stable_sort(singles.begin(), singles.end(), by_len);
+    for (int64_t i : twopass)
+        for (auto& st : B->plans[B->len[i]]->stages) smax = std::max(smax, st.smem);
+    for (int64_t i : singles) smax = std::max(smax, batched_smem(B->plans[B->len[i]]->stages[0]));
+    const void* fn = cfft_queue_kernel(dt, mb);
+    CUDA_TRY(cfft_prepare_fn(fn, smax, 1));
+    int per_sm = 0, nsm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, CFFT_THREADS, smax));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, B->device));
+    if (per_sm < 1) return fail(CFFT_ERR_UNSUPPORTED, "the batch's queue kernel does not fit an SM");
+    const int resident = per_sm * nsm;
+
+    // Two-pass transforms, largest first, in slabs: consecutive transforms
+    // whose scratch fits one slot of a ring, closed once a stage holds at
+    // least two waves of tiles.  The items run as a software pipeline of
+    // steps: step t holds stage 3 of slab t-3, stage 2 of slab t-2, stage 1
+    // of slab t-1 and stage 0 of slab t, so an item's dependency (the
+    // previous stage of its transform) was handed out a step earlier, and
+    // the intermediate it reads was written recently (L2).  A slab first
+    // waits for the slab that last used its slot; single-CTA transforms are
+    // spread over the steps (no dependencies: they fill the waits).
+    auto scratch_need = [&](int64_t i) {
+        cfft_plan_s* P = B->plans[B->len[i]];
+        return (size_t)P->shape.M * e * (P->stages.size() > 2 ? 2 : 1);
+    };
+    auto stage_tiles = [&](int64_t i, int s) { return blocks_for(B->plans[B->len[i]]->stages[s].kp); };
+    std::vector<std::vector<int64_t>> slabs;
+    size_t slot = 0;
+    int nslots = 1;
+    if (!twopass.empty()) {
+        size_t total = 0, need_max = 0;
+        for (int64_t i : twopass) {
+            total += scratch_need(i);
+            need_max = std::max(need_max, scratch_need(i));
+        }
+        slot = std::max(need_max, (size_t)scratch_budget());
+        size_t used = 0;
+        int64_t tiles = 0;
+        slabs.emplace_back();
+        for (int64_t i : twopass) {
+            if (!slabs.back().empty() && (used + scratch_need(i) > slot || tiles >= 2 * resident)) {
+                slabs.emplace_back();
+                used = 0;
+                tiles = 0;
+            }
+            slabs.back().push_back(i);
+            used += scratch_need(i);
+            tiles += stage_tiles(i, 0);
+        }
+        size_t freeb = 0, totb = 0;
+        cudaMemGetInfo(&freeb, &totb);
+        // the pipeline keeps four slabs in flight: six slots (or as many as
+        // the slabs, or as a quarter of free memory holds, at least four)
+        nslots = (int)std::min<size_t>(slabs.size(), std::max<size_t>(4, std::min<size_t>(6, freeb / 4 / slot)));
+        if (slabs.size() == 1) slot = total;
+        CUDA_TRY(lib_malloc(&B->scratch[0], slot * nslots));
+        B->allocs.push_back(B->scratch[0]);
+    }
+    const int nslabs = (int)slabs.size();
+    const int nsteps = nslabs ? nslabs + 3 : 1;
+    std::vector<int> slab_ctr(nslabs), slab_need(nslabs, 0);
+    for (int k = 0; k < nslabs; k++) slab_ctr[k] = nctr++;
+    std::map<int64_t, std::pair<int64_t, int64_t>> so;   // scratch offsets (elements) in the slab's slot
+    std::map<int64_t, std::vector<int>> sctr;            // stage counters per transform
+    for (int k = 0; k < nslabs; k++) {
+        int64_t cur = 0;
+        for (int64_t i : slabs[k]) {
+            cfft_plan_s* P = B->plans[B->len[i]];
+            const int64_t M = P->shape.M;
+            so[i] = {cur, P->stages.size() > 2 ? cur + M : -1};
+            cur += M * (P->stages.size() > 2 ? 2 : 1);
+        }
+    }
+    auto emit_stage = [&](int k, int64_t i, int pass) {
+        cfft_plan_s* P = B->plans[B->len[i]];
+        const int ns = (int)P->stages.size();
+        const Stage& st = P->stages[pass];
+        char* base = (char*)B->scratch[0] + (size_t)(k % nslots) * slot;
+        KParams kp = st.kp;
+        kp.batch = 1;
+        kp.scale = 1.0 / (double)B->len[i];
+        auto where = [&](int sel, const void** ptr, long long* off, unsigned char* user, long long* dist) {
+            if (sel <= 1) {
+                *ptr = nullptr;
+                *off = B->off[i];
+                *user = 1;
+                *dist = B->len[i];
+            } else {
+                const int64_t o = (sel == 2) ? so[i].first : so[i].second;
+                *ptr = base + (size_t)o * e;
+                *off = 0;
+                *user = 0;
+                *dist = P->shape.M;
+            }
+        };
+        const void *ip, *op;
+        where(st.in_sel, &ip, &kp.in_off, &kp.in_user, &kp.in_dist);
+        where(st.out_sel, &op, &kp.out_off, &kp.out_user, &kp.out_dist);
+        kp.in = ip;
+        kp.out = (void*)op;
+        const int tiles = blocks_for(kp);
+        int wait = -1, need = 0;
+        if (pass == 0) {
+            if (k >= nslots) {
+                wait = slab_ctr[k - nslots];
+                need = slab_need[k - nslots];
+            }
+        } else {
+            wait = sctr[i][pass - 1];
+            need = stage_tiles(i, pass - 1);
+        }
+        int done;
+        if (pass == ns - 1) {
+            done = slab_ctr[k];
+            slab_need[k] += tiles;
+        } else {
+            done = nctr++;
+            sctr[i].push_back(done);
+        }
+        const int kind = kp.mode == MODE_COLPASS ? QK_COLPASS : QK_ROWPASS;
+        const int d = (int)desc.size();
+        desc.push_back(kp);
+        for (int b = 0; b < tiles; b++) items.push_back({d, b, kind, wait, need, done});
+    };
+    auto emit_single = [&](int64_t i) {
+        cfft_plan_s* P = B->plans[B->len[i]];
+        KParams kp = P->stages[0].kp;
+        const void* vf = batched_variant(kp, dtype);
+        const int kind = kp.mode == MODE_ROWS ? QK_ROWS
+                         : vf == cfft_batch_kernel_for(MODE_FOUR_WARP, dt) ? QK_FOUR_WARP : QK_FOUR;
+        kp.batch = 1;
+        kp.in_off = kp.out_off = B->off[i];
+        kp.in_user = kp.out_user = 1;
+        kp.in_dist = kp.out_dist = B->len[i];
+        kp.scale = 1.0 / (double)B->len[i];
+        const int d = (int)desc.size();
+        desc.push_back(kp);
+        const int nb = blocks_for(kp);
+        for (int b = 0; b < nb; b++) items.push_back({d, b, kind, -1, 0, -1});
+    };
+    size_t next_single = 0;
+    for (int t = 0; t < nsteps; t++) {
+        for (int s = 3; s >= 0; s--) {
+            const int k = t - s;
+            if (k < 0 || k >= nslabs) continue;
+            for (int64_t i : slabs[k])
+                if (s < (int)B->plans[B->len[i]]->stages.size()) emit_stage(k, i, s);
+        }
+        // this step's share of the single-CTA transforms
+        const size_t upto = singles.size() * (size_t)(t + 1) / (size_t)nsteps;
+        for (; next_single < upto; next_single++) emit_single(singles[next_single]);
+    }
+    B->qfn = fn;
+    void *dd = nullptr, *di = nullptr, *dc = nullptr;
+    CUDA_TRY(lib_malloc(&dd, desc.size() * sizeof(KParams)));
+    B->allocs.push_back(dd);
+    CUDA_TRY(lib_malloc(&di, items.size() * sizeof(QItem)));
+    B->allocs.push_back(di);
+    CUDA_TRY(lib_malloc(&dc, (size_t)(2 + nctr) * sizeof(int)));
+    B->allocs.push_back(dc);
+    CUDA_TRY(cudaMemcpy(dd, desc.data(), desc.size() * sizeof(KParams), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(di, items.data(), items.size() * sizeof(QItem), cudaMemcpyHostToDevice));
+    B->queue = true;
+    B->q_desc = (KParams*)dd;
+    B->q_items = (QItem*)di;
+    B->q_ctl = (int*)dc;
+    B->q_nitems = (int)items.size();
+    B->q_nctl = 2 + nctr;
+    B->q_smem = smax;
+    B->q_grid = (unsigned)B->q_nitems;              // one CTA per work item
+    CUDA_TRY(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
+    return CFFT_OK;
+}
+
 static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* lengths, int dtype, int flags) {
     const size_t e = elem_bytes(dtype);
     B->dtype = dtype;
@@ -1857,6 +2124,7 @@ static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* leng
         acc += lengths[i];
     }
     B->total = acc;
+    if (!(flags & CFFT_BATCH_GROUPED)) return batch_create_queue(B);
     // one plan per distinct length (batch 1, scratch shared by the batch)
     for (int64_t n : B->len) {
         if (B->plans.count(n)) continue;
@@ -1980,6 +2248,21 @@ static int batch_create_impl(cfft_batch_s* B, int64_t count, const int64_t* leng
 }
 
 static int batch_enqueue(cfft_batch_s* B, const void* in, void* out, int dir, cudaStream_t st) {
+    if (B->queue) {
+        CUDA_TRY(cudaMemsetAsync(B->q_ctl, 0, (size_t)B->q_nctl * sizeof(int), st));
+        QueueLaunch L;
+        L.desc = B->q_desc;
+        L.items = B->q_items;
+        L.in_base = in;
+        L.out_base = out;
+        L.ctl = B->q_ctl;
+        L.nitems = B->q_nitems;
+        L.dir = dir;
+        cudaError_t ce = cfft_launch_queue(B->qfn, L, B->q_grid, B->q_smem, st);
+        if (ce != cudaSuccess) return fail(CFFT_ERR_CUDA, std::string("batched launch: ") + cudaGetErrorString(ce));
+        B->launches = 1;
+        return CFFT_OK;
+    }
     int launches = 0;
     for (auto* list : {&B->groups, &B->passes}) {
         for (auto& g : *list) {
@@ -2772,7 +3055,7 @@ int64_t cfft_batch_elements(cfft_batch batch) { return batch ? batch->total : -1
 
 int cfft_batch_launches(cfft_batch batch) {
     if (!batch) return -1;
-    return (int)(batch->groups.size() + batch->passes.size());
+    return batch->queue ? 1 : (int)(batch->groups.size() + batch->passes.size());
 }
 
 int cfft_plan_launches(cfft_plan plan) {

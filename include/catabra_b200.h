@@ -41,8 +41,10 @@ enum { CFFT_FORWARD = 0, CFFT_INVERSE = 1, CFFT_BACKWARD = 2 };
  * NO_FLAG = heuristic plan, MEASURE = time candidate plans on the device,
  * ENCHANT = wider timed search (factorisations x cluster sizes x radix
  * orders).  Bit 4 (CFFT_EXACT_TWIDDLES) replaces the reference's Rader
- * twiddle recurrence (src/prime.jl:36-37) by exactly rounded twiddles. */
-enum { CFFT_NO_FLAG = 0, CFFT_MEASURE = 1, CFFT_ENCHANT = 2, CFFT_EXACT_TWIDDLES = 16 };
+ * twiddle recurrence (src/prime.jl:36-37) by exactly rounded twiddles.
+ * Bit 5 (CFFT_BATCH_GROUPED, cfft_batch_create only) selects the grouped
+ * schedule of the batched form instead of its single queue launch. */
+enum { CFFT_NO_FLAG = 0, CFFT_MEASURE = 1, CFFT_ENCHANT = 2, CFFT_EXACT_TWIDDLES = 16, CFFT_BATCH_GROUPED = 32 };
 
 /* status codes */
 enum {
@@ -116,9 +118,15 @@ int cfft_plan_launches(cfft_plan plan);
  * the order given (transform i starts at element sum(lengths[:i])).  The
  * reference transforms one vector per call (fft_kernel!, src/kernel.jl:95-100,
  * with one cached function per length); this plans every distinct length
- * once and runs the whole batch as one CUDA graph: single-kernel transforms
- * grouped into a few descriptor-driven launches, largest first, the rest on
- * a shared scratch.  flags: CFFT_EXACT_TWIDDLES only. */
+ * once and runs the whole batch as one CUDA graph holding one kernel
+ * launch: its CTAs claim work items by atomic ticket (whole single-CTA
+ * transforms, and the tiles of two-pass transforms, whose stages wait for
+ * one another through counters with bounded waits) from a queue built
+ * here, largest transforms first.  A wait that runs out stops the launch and sets bit 1
+ * of cfft_device_faults.  With CFFT_BATCH_GROUPED the graph instead holds
+ * grouped descriptor-driven launches (single-kernel transforms by kernel
+ * variant, cluster size and shared-memory class; two-pass transforms pass by
+ * pass on a shared scratch).  flags: CFFT_EXACT_TWIDDLES, CFFT_BATCH_GROUPED. */
 typedef struct cfft_batch_s* cfft_batch;
 int cfft_batch_create(cfft_batch* batch, int64_t count, const int64_t* lengths, int dtype, int flags);
 
