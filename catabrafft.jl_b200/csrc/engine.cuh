@@ -293,14 +293,37 @@ template <typename V>
 __device__ __forceinline__ V r4096_tw(V v, const double2* lo, const double2* hi, unsigned e) {
     return e ? cmul(v, fromd<V>(r4096_w(lo, hi, e))) : v;
 }
+// dst[k stride] = v[k] w_4096^(e0 k), k < 16 (e0 k < 4096).  ComplexF64:
+// each twiddle from the two-level table (one FP64 product of exactly rounded
+// entries), applied as it is stored.  ComplexF32: the FP64 powers
+// w^(e0 k) = w^(e0 (k-1)) w^e0 of one table value, each rounded once to
+// FP32 (the FP64 power's relative error stays near 1e-15, far below the
+// rounding); the table reads this saves were most of the ComplexF32
+// kernel's shared-memory traffic.
+template <typename V>
+__device__ __forceinline__ void r4096_tw_store(V (&v)[16], V* dst, int stride, const double2* lo,
+                                               const double2* hi, unsigned e0) {
+    if constexpr (sizeof(V) == sizeof(float2)) {
+        const double2 b = r4096_w(lo, hi, e0);
+        double2 w = b;
+        dst[0] = v[0];
+#pragma unroll
+        for (int k = 1; k < 16; k++) {
+            dst[k * stride] = cmul(v[k], fromd<V>(w));
+            if (k < 15) w = cmul(w, b);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) dst[k * stride] = r4096_tw(v[k], lo, hi, e0 * (unsigned)k);
+    }
+}
 // 4096-point DFT of the registers: thread t holds x[t + 256 k] in v[k] and
 // gets X[t + 256 k3] in v[k3].  buf (16 planes of R4096_PL elements) must be
 // free on entry; on return every thread has finished reading it.
 template <typename V>
 __device__ __forceinline__ void fft4096_regs(V (&v)[16], V* buf, const double2* tlo, const double2* thi, int t) {
     dft<16>(v);
-#pragma unroll
-    for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = r4096_tw(v[k1], tlo, thi, (unsigned)(t * k1));
+    r4096_tw_store(v, buf + t, 256, tlo, thi, (unsigned)t);
     __syncthreads();
     {
         const int t1 = t & 15, k1 = t >> 4;
@@ -308,9 +331,7 @@ __device__ __forceinline__ void fft4096_regs(V (&v)[16], V* buf, const double2* 
         for (int t2 = 0; t2 < 16; t2++) v[t2] = buf[k1 * 256 + t1 + 16 * t2];
         dft<16>(v);
         __syncthreads();                        // every Y read before Z overwrites it
-#pragma unroll
-        for (int k2 = 0; k2 < 16; k2++)
-            buf[k1 * R4096_PL + k2 * R4096_PB + t1] = r4096_tw(v[k2], tlo, thi, (unsigned)(16 * t1 * k2));
+        r4096_tw_store(v, buf + k1 * R4096_PL + t1, R4096_PB, tlo, thi, (unsigned)(16 * t1));
     }
     __syncthreads();
     {
@@ -404,8 +425,7 @@ __device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem
 #pragma unroll
         for (int k = 0; k < 16; k++) v[k] = load_in(p, buf[t + 256 * k]);
         dft<16>(v);
-#pragma unroll
-        for (int k1 = 0; k1 < 16; k1++) buf[k1 * 256 + t] = r4096_tw(v[k1], tlo, thi, (unsigned)(t * k1));
+        r4096_tw_store(v, buf + t, 256, tlo, thi, (unsigned)t);
         if (TMA) {
             // every thread leaves together when a copy timed out
             if (__syncthreads_or(!ok)) {
@@ -421,9 +441,7 @@ __device__ __forceinline__ void r4096_body(const KParams& p, unsigned char* smem
             for (int t2 = 0; t2 < 16; t2++) v[t2] = buf[k1 * 256 + t1 + 16 * t2];
             dft<16>(v);
             __syncthreads();                    // every Y read before Z overwrites it
-#pragma unroll
-            for (int k2 = 0; k2 < 16; k2++)
-                buf[k1 * R4096_PL + k2 * R4096_PB + t1] = r4096_tw(v[k2], tlo, thi, (unsigned)(16 * t1 * k2));
+            r4096_tw_store(v, buf + k1 * R4096_PL + t1, R4096_PB, tlo, thi, (unsigned)(16 * t1));
         }
         __syncthreads();
         {
