@@ -33,36 +33,44 @@ def _mtime(p: str) -> float:
     return os.path.getmtime(p) if os.path.exists(p) else 0.0
 
 
+def _obj(s: str) -> str:
+    return os.path.join(HERE, "_build", s + ".o")
+
+
+def _stale_objects(force: bool) -> list:
+    """Sources whose object is missing or older than the source or any header
+    (a source edited while a build runs stays stale: the check is per object,
+    not against the library)."""
+    hdr = max(_mtime(h) for h in _headers())
+    out = []
+    for s in DEVICE_SOURCES + HOST_SOURCES:
+        if force or _mtime(_obj(s)) <= max(hdr, _mtime(os.path.join(CSRC, s))):
+            out.append(s)
+    return out
+
+
 def _stale() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    paths = [os.path.join(CSRC, s) for s in DEVICE_SOURCES + HOST_SOURCES] + _headers()
-    return any(_mtime(p) > t for p in paths)
+    objs = [_obj(s) for s in DEVICE_SOURCES + HOST_SOURCES]
+    return bool(_stale_objects(False)) or not os.path.exists(LIB) or \
+        any(_mtime(o) > _mtime(LIB) for o in objs)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile the objects whose source or any header changed (all of them
     with force), then link the library."""
-    if not force and not _stale():
+    todo = _stale_objects(force)
+    if not todo and not _stale():
         return LIB
-    objdir = os.path.join(HERE, "_build")
-    os.makedirs(objdir, exist_ok=True)
-    hdr = max(_mtime(h) for h in _headers())
-    objs = []
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC]
-    for s in DEVICE_SOURCES + HOST_SOURCES:
-        src = os.path.join(CSRC, s)
-        o = os.path.join(objdir, s + ".o")
-        objs.append(o)
-        if not force and _mtime(o) > max(hdr, _mtime(src)):
-            continue
-        cmd = [NVCC, *ARCH, *common, "-c", src, "-o", o]
+    for s in todo:
+        cmd = [NVCC, *ARCH, *common, "-c", os.path.join(CSRC, s), "-o", _obj(s)]
         if s in DEVICE_SOURCES:
             cmd.insert(3, "-lineinfo")
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)
+    objs = [_obj(s) for s in DEVICE_SOURCES + HOST_SOURCES]
     tmp = LIB + ".tmp"
     subprocess.run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)

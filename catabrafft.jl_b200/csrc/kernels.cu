@@ -172,6 +172,13 @@ __global__ void __launch_bounds__(CFFT_THREADS, MB) k_p2row_tma(const __grid_con
     extern __shared__ __align__(128) unsigned char smem[];
     r4096_body<double2, R4096_P2A_TMA>(p, smem, &tm);
 }
+// pass A for ComplexF32 with tensor copies of subsequence pairs (two CTAs
+// per SM: 64 KB of pair buffer + the exchange buffer): tm maps the chunk's
+// input as [transform][c < 4096][2 N1 floats] (strides N1 x 8 B, in_dist x 8 B)
+__global__ void __launch_bounds__(CFFT_THREADS, 2) k_p2row_tma2(const __grid_constant__ CUtensorMap tm, KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    p2row_pair_body(p, smem, &tm);
+}
 template <typename V, int MB> static const void* p2col_for(int N1) {
     switch (N1) {
         case 2: return (const void*)k_p2col<V, 2, MB>;
@@ -255,6 +262,8 @@ cudaError_t cfft_launch_p2flow(const void* f, const KParams& pa, const KParams& 
 const void* cfft_p2row_tma_kernel(int mb) {
     return mb == 2 ? (const void*)k_p2row_tma<2> : (const void*)k_p2row_tma<3>;
 }
+const void* cfft_p2row_tma2_kernel() { return (const void*)k_p2row_tma2; }
+size_t cfft_p2row_tma2_smem() { return (size_t)kP2PairBytes + cfft_r4096_smem(sizeof(float2)); }
 // the driver's tensor-map encoder, looked up once through the runtime
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -281,6 +290,35 @@ cudaError_t cfft_launch_p2row_tma(const void* f, const KParams& p, unsigned grid
     // L2 promotion to 256 B: the neighbouring subsequences of the same
     // lines are read by the CTAs working on the next rows
     CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)p.in, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(CFFT_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    KParams pc = p;
+    void* args[] = {(void*)&tm, (void*)&pc};
+    cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
+cudaError_t cfft_launch_p2row_tma2(const void* f, const KParams& p, unsigned grid, size_t smem, cudaStream_t st) {
+    auto enc = tensor_map_encoder();
+    if (!f || !enc) return cudaErrorNotSupported;
+    const int N1 = 1 << p.PA;
+    const long long nb = (long long)p.batch >> p.PA;
+    // pairs of subsequences: N1 even, rows a multiple of 2; 16-byte aligned
+    // base and strides (N1 x 8 B, in_dist x 8 B)
+    if (N1 < 2 || (p.batch & 1) || nb < 1 || nb > 0x7fffffffLL || ((uintptr_t)p.in & 15) || (p.in_dist & 1))
+        return cudaErrorInvalidValue;
+    CUtensorMap tm;
+    const cuuint64_t dims[3] = {(cuuint64_t)(2 * N1), 4096, (cuuint64_t)nb};
+    const cuuint64_t strides[2] = {(cuuint64_t)N1 * 8, (cuuint64_t)p.in_dist * 8};
+    const cuuint32_t box[3] = {4, 256, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)p.in, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;

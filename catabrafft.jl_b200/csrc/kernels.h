@@ -45,6 +45,11 @@ cudaError_t cfft_launch_p2flow(const void* fn, const KParams& pa, const KParams&
 // tensor map of p.in for this launch)
 const void* cfft_p2row_tma_kernel(int mb);
 cudaError_t cfft_launch_p2row_tma(const void* fn, const KParams& p, unsigned grid, size_t smem, cudaStream_t st);
+// ComplexF32 pass A with tensor copies of subsequence pairs (two CTAs per
+// SM; batch = rows, even), its shared memory and launcher
+const void* cfft_p2row_tma2_kernel();
+size_t cfft_p2row_tma2_smem();
+cudaError_t cfft_launch_p2row_tma2(const void* fn, const KParams& p, unsigned grid, size_t smem, cudaStream_t st);
 // Rader for primes on a cluster of C in {3, 4, 5, 7, 8} register 4096-point
 // CTAs (convc.cuh; M = 4096 C), built for mb = 3 or 2 CTAs per SM
 // (ComplexF64; ComplexF32 is always 3), and its shared memory

@@ -24,8 +24,8 @@
 // shared accesses are runs of consecutive 16-byte slots, and the last stage's
 // stride-R2 reads are conflict-free for an odd R2.  Stage 0's inputs arrive
 // by cp.async in the slots the same thread reads and then overwrites, so the
-// load needs no barrier.  Twiddles: FP64 two-level tables of w_L and w_n in
-// shared memory, each product rounded once to the data type.
+// load needs no barrier.  Twiddles: FP64 powers of values from two-level
+// tables of w_L and w_n in shared memory, each rounded once to the data type.
 #pragma once
 #include "engine.cuh"
 
@@ -41,10 +41,36 @@ template <int C_, int R0_, int R1_, int R2_, int T_> struct MixShape {
     static_assert(R2 % 2 == 1, "the last stage's stride-R2 reads are conflict-free for odd R2");
 };
 
-// x w^e from a two-level FP64 table staged in shared memory
-template <typename V>
-__device__ __forceinline__ V mx_tw(V v, const double2* lo, const double2* hi, int bits, unsigned e) {
-    return e ? cmul(v, fromd<V>(cmul(lo[e & ((1u << bits) - 1)], hi[e >> bits]))) : v;
+// w^e from a two-level FP64 table
+__device__ __forceinline__ double2 mx_w(const double2* lo, const double2* hi, int bits, unsigned e) {
+    return cmul(lo[e & ((1u << bits) - 1)], hi[e >> bits]);
+}
+// v[k] w^(e0 k) for k < R, stored at dst[k stride] (mx_tw_store) or kept in
+// place (mx_tw_row): the FP64 powers w^(e0 k) = w^(e0 (k-1)) w^e0 of one
+// table value, each rounded once to V (the same FP64 work as a table
+// product per twiddle, without the per-twiddle table reads; the powers'
+// relative error stays near 1e-15)
+template <int R, typename V>
+__device__ __forceinline__ void mx_tw_store(const V* v, V* dst, int stride, const double2* lo, const double2* hi,
+                                            int bits, unsigned e0) {
+    const double2 b = mx_w(lo, hi, bits, e0);
+    double2 w = b;
+    dst[0] = v[0];
+#pragma unroll
+    for (int k = 1; k < R; k++) {
+        dst[k * stride] = cmul(v[k], fromd<V>(w));
+        if (k < R - 1) w = cmul(w, b);
+    }
+}
+template <int R, typename V>
+__device__ __forceinline__ void mx_tw_row(V* v, const double2* lo, const double2* hi, int bits, unsigned e0) {
+    const double2 b = mx_w(lo, hi, bits, e0);
+    double2 w = b;
+#pragma unroll
+    for (int k = 1; k < R; k++) {
+        v[k] = cmul(v[k], fromd<V>(w));
+        if (k < R - 1) w = cmul(w, b);
+    }
 }
 
 // KParams: t4 = two-level table of w_L, t4n = two-level table of w_n (both
@@ -91,10 +117,7 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
             dft<S::R0>(*reinterpret_cast<V(*)[S::R0]>(v));
         }
         __syncthreads();                        // tables staged (the slots are this thread's own)
-        if (b < S::NB0) {
-#pragma unroll
-            for (int k = 0; k < S::R0; k++) buf[b + S::NB0 * k] = mx_tw(v[k], llo, lhi, bl, (unsigned)(b * k));
-        }
+        if (b < S::NB0) mx_tw_store<S::R0>(v, buf + b, S::NB0, llo, lhi, bl, (unsigned)b);
         __syncthreads();
     }
     {
@@ -108,9 +131,7 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
         __syncthreads();                        // every read before the writes
         if (b < S::NBF1) {
             dft<S::R1>(*reinterpret_cast<V(*)[S::R1]>(v));
-#pragma unroll
-            for (int k = 0; k < S::R1; k++)
-                buf[(K + S::R0 * k) * S::NB1 + tp] = mx_tw(v[k], llo, lhi, bl, (unsigned)(tp * k * S::R0));
+            mx_tw_store<S::R1>(v, buf + K * S::NB1 + tp, S::R0 * S::NB1, llo, lhi, bl, (unsigned)(tp * S::R0));
         }
         __syncthreads();
     }
@@ -137,8 +158,7 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
             V f[S::C];
 #pragma unroll
             for (int q = 0; q < S::C; q++) f[q] = cl.map_shared_rank(buf, q)[k];
-#pragma unroll
-            for (int q = 1; q < S::C; q++) f[q] = mx_tw(f[q], glo, ghi, bn, (unsigned)(q * k));
+            mx_tw_row<S::C>(f, glo, ghi, bn, (unsigned)k);
             dft<S::C>(f);
 #pragma unroll
             for (int q = 0; q < S::C; q++) stg_stream(out + k + S::L * q, store_out(p, f[q]));

@@ -272,7 +272,7 @@ struct Stage {
     int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
     size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
     unsigned persist = 0;    // kernels that loop over the batch: CTAs to launch at most
-    int launch = 0;          // 1: pass A by tensor copies (its own launcher); 2: dataflow launch
+    int launch = 0;          // 1 / 3: pass A by tensor copies (ComplexF64 / ComplexF32 pairs); 2: dataflow launch
     KParams kp2;             // dataflow launch: the pass-B parameters
     int flow_lag = 0, flow_depth = 0;
 };
@@ -536,7 +536,9 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     }
     for (int c = 0; c < 4; c++) {
         const int var = ((c < 2) == tma_first) ? 1 : 0, mb = (c % 2 == 0) ? 3 : 2;
-        if (dtype != CFFT_C128 && (var == 1 || mb == 2)) continue;
+        // ComplexF32: pass A by cp.async at three CTAs per SM, or by tensor
+        // copies of subsequence pairs at two
+        if (dtype != CFFT_C128 && mb != (var == 1 ? 2 : 3)) continue;
         Shape s;
         s.var = var;
         s.mode = MODE_P2COL;
@@ -1328,6 +1330,12 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         a.out_sel = 2;
         a.fn = sh.var == 1 ? cfft_p2row_tma_kernel(mb) : cfft_p2row_kernel(P->dtype, mb);
         a.launch = sh.var == 1 ? 1 : 0;
+        if (sh.var == 1 && P->dtype != CFFT_C128) {
+            // ComplexF32: subsequence pairs per tensor-copy item
+            a.fn = cfft_p2row_tma2_kernel();
+            a.smem = cfft_p2row_tma2_smem();
+            a.launch = 3;
+        }
         Stage b;
         b.kp = kp;
         b.kp.mode = MODE_P2COL;
@@ -1524,6 +1532,8 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
                                             s.flow_depth, s.persist, s.smem, st);
             } else if (s.launch == 1) {
                 ce = cfft_launch_p2row_tma(s.fn, kp, grid, s.smem, st);
+            } else if (s.launch == 3) {
+                ce = cfft_launch_p2row_tma2(s.fn, kp, grid, s.smem, st);
             } else {
                 ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             }

@@ -182,6 +182,79 @@ __device__ __forceinline__ void p2col_stages(const KParams& p, V* buf, const dou
 // p.t4n = the two-level table of w_n (staged after it when p.pre != 0).
 // Pass A conjugated the input of the inverse directions; the stores here
 // conjugate and scale.
+// Pass A for ComplexF32 by tensor copies.  The 8-byte elements are narrower
+// than a tensor copy's 16-byte minimum box row, so a CTA item is the pair of
+// neighbouring subsequences (i, i + 1), i even, of one transform: 16 copies
+// of a box of 256 columns x 16 bytes bring both, side by side (64 KB), onto
+// an mbarrier.  Each subsequence then runs the 4096-point register FFT
+// through the exchange buffer and is written, unscaled, as its row 2 b + h
+// of the intermediate (row = transform x N1 + i, as in R4096_P2A).  The next
+// pair's copies are issued as soon as every thread has read the second
+// subsequence.  (Per-element cp.async of the strided input writes shared
+// memory one sector at a time: most of the ComplexF32 pass's shared-memory
+// traffic.)  KParams as for R4096_P2A: batch = rows (even), PA = log2 N1.
+constexpr int kP2PairBytes = 4096 * 16;
+__device__ __forceinline__ void p2row_pair_issue(const KParams& p, float4* pair, const CUtensorMap* tm,
+                                                 uint64_t* bar, int pb) {
+    const int sh = p.PA - 1;                    // pairs per transform: N1 / 2
+    const int tt = pb >> sh, i = (pb & ((1 << sh) - 1)) << 1;
+    mbar_expect_tx(bar, kP2PairBytes);
+#pragma unroll
+    for (int k = 0; k < 16; k++) tma_load_3d(pair + 256 * k, tm, bar, 2 * i, 256 * k, tt);
+}
+__device__ __forceinline__ void p2row_pair_body(const KParams& p, unsigned char* smem, const CUtensorMap* tm) {
+    float4* pair = (float4*)smem;
+    float2* buf = (float2*)(smem + kP2PairBytes);  // 16 planes of R4096_PL elements
+    double2* tlo = after16(buf + 16 * R4096_PL);
+    double2* thi = tlo + 64;
+    uint64_t* bar = (uint64_t*)(thi + 65);
+    const int npairs = p.batch >> 1;
+    int b = block_id(p);
+    if (b >= npairs) return;                    // uniform across the CTA
+    {
+        const int t = opaque_tid();
+        if (t == 0) mbar_init(bar, 1);
+        if (t < 64) tlo[t ^ (t >> 3)] = p.t4.lo[t];
+        if (t < 65) thi[t] = p.t4.hi[t];
+        __syncthreads();                        // the barrier is initialised, the tables staged
+        if (t == 0) p2row_pair_issue(p, pair, tm, bar, b);
+    }
+    unsigned phase = 0;
+    for (; b < npairs; b += gridDim.x) {
+        {
+            const bool ok = mbar_wait(bar, phase);  // the pair's tensor copies have landed
+            phase ^= 1;
+            // every thread leaves together when a copy timed out
+            if (__syncthreads_or(!ok)) {
+                if (opaque_tid() == 0) record_fault(kFaultTmaTimeout);
+                return;
+            }
+        }
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            const int t = opaque_tid();
+            float2 v[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const float4 q = pair[t + 256 * k];
+                v[k] = load_in(p, h ? make_float2(q.z, q.w) : make_float2(q.x, q.y));
+            }
+            if (h == 1) {
+                __syncthreads();                // both subsequences read: the pair buffer is free
+                const int bn = b + (int)gridDim.x;
+                if (t == 0 && bn < npairs) {
+                    fence_proxy_async_smem();   // the reads above precede the copies' writes
+                    p2row_pair_issue(p, pair, tm, bar, bn);
+                }
+            }
+            fft4096_regs(v, buf, tlo, thi, t);
+            float2* out = (float2*)p.out + (long long)(2 * b + h) * p.out_dist;
+#pragma unroll
+            for (int k3 = 0; k3 < 16; k3++) out[t + 256 * k3] = v[k3];
+        }
+    }
+}
+
 template <typename V, int N1>
 __device__ __forceinline__ void p2col_body(const KParams& p, unsigned char* smem) {
     using PC = P2Col<N1>;

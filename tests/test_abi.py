@@ -85,7 +85,7 @@ def test_strategy_choice(n, expect):
 
 
 @pytest.mark.parametrize("n,expect", [
-    (65536, "pow2(N1=16,N2=4096,ctas_per_sm=3)"), (8192, "pow2cluster(C=2,4096 per CTA,ctas_per_sm=2)"), (1 << 17, "pow2(N1=32,N2=4096,ctas_per_sm=3)"), (19683, "four(C="), (4096, "rows"),
+    (65536, "pow2(N1=16,N2=4096,ctas_per_sm=2,tma)"), (8192, "pow2cluster(C=2,4096 per CTA,ctas_per_sm=2)"), (1 << 17, "pow2(N1=32,N2=4096,ctas_per_sm=2,tma)"), (19683, "four(C=3,"), (4096, "rows"),
 ])
 def test_strategy_choice_complex64(n, expect):
     m = load()

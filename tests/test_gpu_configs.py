@@ -202,7 +202,8 @@ def test_pow2_register_passes(cb, dtype):
     kernel over the stride-N1 subsequences; ComplexF64 loads them by tensor
     copies) and pass B (the N1-point column DFTs).  Batches give every
     persistent CTA several rows and tiles (prefetch into the freed buffer),
-    and the largest lengths run several intermediate chunks.  Forward,
+    and the largest lengths run several intermediate chunks.  ComplexF32
+    takes pass A by tensor copies of subsequence pairs.  Forward,
     inverse, backward and in place against the oracle; no kernel recorded a
     timed-out wait."""
     cb._lib.LIB.cfft_device_faults(1)
@@ -213,8 +214,8 @@ def test_pow2_register_passes(cb, dtype):
         if n <= 16384:                              # one pass on a cluster of N1 CTAs
             _pow2_check(cb, n, batch, dtype, f"pow2cluster(C={N1},4096 per CTA,ctas_per_sm=2)")
         else:
-            tag = ",tma)" if dtype == np.complex128 else ")"
-            _pow2_check(cb, n, batch, dtype, f"pow2(N1={N1},N2=4096,ctas_per_sm=3{tag}")
+            shape = "ctas_per_sm=3,tma)" if dtype == np.complex128 else "ctas_per_sm=2,tma)"
+            _pow2_check(cb, n, batch, dtype, f"pow2(N1={N1},N2=4096,{shape}")
     assert cb._lib.LIB.cfft_device_faults(1) == 0
 
 
@@ -240,6 +241,35 @@ def test_pow2_other_variants(cb, tmp_path):
         try:
             for n, batch in cases:
                 _pow2_check(cb, n, batch, np.complex128, f"pow2(N1={n // 4096},N2=4096,ctas_per_sm={mb}{tag}",
+                            flags=cb.MEASURE)
+        finally:
+            cb.forget_wisdom()
+    assert cb._lib.LIB.cfft_device_faults(1) == 0
+
+
+def test_pow2_c64_pass_a_variants(cb, tmp_path):
+    """Both ComplexF32 builds of pass A through wisdom entries for MEASURE
+    plans: per-element cp.async at three CTAs per SM, and tensor copies of
+    subsequence pairs at two (64 KB pair buffer; N1 = 2 is a single pair per
+    transform), against the oracle at 1e-5."""
+    variants = [(3, 0, ")"), (2, 1, ",tma)")]
+    cases = [(1 << 13, 120), (1 << 15, 40), (1 << 16, 21), (1 << 20, 3), (1 << 22, 2)]
+    cb._lib.LIB.cfft_device_faults(1)
+    for mb, var, tag in variants:
+        lines = ["catabra-b200-wisdom 1"]
+        for n, batch in cases:
+            N1 = n // 4096
+            sig = f"4 0 {n} {N1} 4096 1 {mb} a {' '.join(map(str, _greedy_split(N1)))} c 16 16 16"
+            if var:
+                sig += f" v{var}"
+            lines.append(f"{n} {batch} {cb.C64} {cb.MEASURE} | {sig}")
+        path = tmp_path / f"c64w{mb}{var}.txt"
+        path.write_text("\n".join(lines) + "\n")
+        cb.forget_wisdom()
+        cb.import_wisdom(str(path))
+        try:
+            for n, batch in cases:
+                _pow2_check(cb, n, batch, np.complex64, f"pow2(N1={n // 4096},N2=4096,ctas_per_sm={mb}{tag}",
                             flags=cb.MEASURE)
         finally:
             cb.forget_wisdom()
