@@ -107,10 +107,13 @@ __device__ __forceinline__ void convc_rader_body(const KParams& p, unsigned char
             V f[C];
 #pragma unroll
             for (int q = 0; q < C; q++) f[q] = cl.map_shared_rank(buf, q)[k];
+            // w_M^(q k) as FP64 powers of one table value (the powers'
+            // relative error stays near 1e-15), each rounded once where used
             double2 w[C];
             w[0] = make_double2(1, 0);
+            w[1] = convc_w(p.t4n, (unsigned)k);
 #pragma unroll
-            for (int q = 1; q < C; q++) w[q] = convc_w(p.t4n, (unsigned)(q * k));
+            for (int q = 2; q < C; q++) w[q] = cmul(w[q - 1], w[1]);
 #pragma unroll
             for (int q = 1; q < C; q++) f[q] = cmul(f[q], fromd<V>(w[q]));
             dft<C>(f);                          // f[q] = A[k + 4096 q]

@@ -384,10 +384,13 @@ __device__ __forceinline__ void p2cl_body(const KParams& p, unsigned char* smem)
             V f[C];
 #pragma unroll
             for (int q = 0; q < C; q++) f[q] = cl.map_shared_rank(buf, q)[k];
+            // w_n^(q k) as FP64 powers of one table value, rounded once
+            const double2 wk = cmul(__ldg(p.t4n.lo + (k & mask)), __ldg(p.t4n.hi + (k >> p.t4n.bits)));
+            double2 w = wk;
 #pragma unroll
             for (int q = 1; q < C; q++) {
-                const unsigned e = (unsigned)(q * k);
-                f[q] = cmul(f[q], fromd<V>(cmul(__ldg(p.t4n.lo + (e & mask)), __ldg(p.t4n.hi + (e >> p.t4n.bits)))));
+                f[q] = cmul(f[q], fromd<V>(w));
+                if (q + 1 < C) w = cmul(w, wk);
             }
             dft<C>(f);
 #pragma unroll
