@@ -26,6 +26,7 @@
 // host and rounded once to the data type.
 #pragma once
 #include <cooperative_groups.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -71,6 +72,39 @@ __device__ __forceinline__ double2 ldg_stream(const double2* p) { return __ldcs(
 __device__ __forceinline__ float2 ldg_stream(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ void stg_stream(double2* p, double2 v) { __stcs(p, v); }
 __device__ __forceinline__ void stg_stream(float2* p, float2 v) { __stcs(p, v); }
+
+// The caller's elements (KParams in_fmt / out_fmt, IO_*): a ComplexF16 or
+// strided plan reads and writes the caller's layout in its first and last
+// kernel, with no widening or gathering sweep of its own.
+template <typename V> __device__ __forceinline__ V from_half(__half2 h);
+template <> __device__ __forceinline__ float2 from_half<float2>(__half2 h) { return __half22float2(h); }
+template <> __device__ __forceinline__ double2 from_half<double2>(__half2 h) {
+    const float2 f = __half22float2(h);
+    return make_double2(f.x, f.y);
+}
+template <typename V> __device__ __forceinline__ __half2 to_half(V v) {
+    return __floats2half2_rn((float)v.x, (float)v.y);
+}
+// element j of transform t of the input
+template <typename V> __device__ __forceinline__ V user_ld(const KParams& p, long long t, long long j) {
+    if (p.in_fmt == IO_PLAIN) return ldg_stream((const V*)p.in + t * p.in_dist + j);
+    const long long off = t * p.in_dist + j * p.in_stride;
+    if (p.in_fmt == IO_HALF) return from_half<V>(((const __half2*)p.in)[off]);
+    return ldg_stream((const V*)p.in + off);
+}
+// ... staged into shared memory: cp.async for contiguous elements, else a
+// load and a shared-memory store (visible after the caller's barrier)
+template <typename V> __device__ __forceinline__ void user_cp(const KParams& p, V* dst, long long t, long long j);
+// element k of transform t of the output
+template <typename V> __device__ __forceinline__ void user_st(const KParams& p, long long t, long long k, V v) {
+    if (p.out_fmt == IO_PLAIN) {
+        stg_stream((V*)p.out + t * p.out_dist + k, v);
+        return;
+    }
+    const long long off = t * p.out_dist + k * p.out_stride;
+    if (p.out_fmt == IO_HALF) ((__half2*)p.out)[off] = to_half(v);
+    else stg_stream((V*)p.out + off, v);
+}
 
 __device__ __forceinline__ double2 tw_two(const TwoLevel& t, unsigned e) {
     // plain loads: the tables may have been staged in shared memory
@@ -124,6 +158,10 @@ template <typename V> __device__ __forceinline__ void cp_async_elem(V* sdst, con
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+template <typename V> __device__ __forceinline__ void user_cp(const KParams& p, V* dst, long long t, long long j) {
+    if (p.in_fmt == IO_PLAIN) cp_async_elem(dst, (const V*)p.in + t * p.in_dist + j);
+    else *dst = user_ld<V>(p, t, j);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
@@ -473,20 +511,34 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
     const int t0 = block_id(p) * p.V;
     const int nrows = min(p.V, p.batch - t0);
     if (nrows <= 0) return;
-    const V* in = (const V*)p.in + (long long)t0 * p.in_dist;
-    V* out = (V*)p.out + (long long)t0 * p.out_dist;
     const int nx = p.nx, M = p.M;
 
     if (p.conv == CONV_NONE) {
-        for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = fdiv(idx, p.mX), i = idx - r * nx;
-            buf[r * p.PC + i] = load_in(p, ldg_stream(in + (long long)r * p.in_dist + i));
+        if (p.in_fmt == IO_PLAIN) {
+            const V* in = (const V*)p.in + (long long)t0 * p.in_dist;
+            for (int idx = tid; idx < nrows * nx; idx += T) {
+                const int r = fdiv(idx, p.mX), i = idx - r * nx;
+                buf[r * p.PC + i] = load_in(p, ldg_stream(in + (long long)r * p.in_dist + i));
+            }
+        } else {
+            for (int idx = tid; idx < nrows * nx; idx += T) {
+                const int r = fdiv(idx, p.mX), i = idx - r * nx;
+                buf[r * p.PC + i] = load_in(p, user_ld<V>(p, t0 + r, i));
+            }
         }
         __syncthreads();
         run_subffts<V, EMAX>(buf, p.pc, nrows, 1, p.PC);
-        for (int idx = tid; idx < nrows * nx; idx += T) {
-            const int r = fdiv(idx, p.mX), i = idx - r * nx;
-            stg_stream(out + (long long)r * p.out_dist + i, store_out(p, buf[r * p.PC + i]));
+        if (p.out_fmt == IO_PLAIN) {
+            V* out = (V*)p.out + (long long)t0 * p.out_dist;
+            for (int idx = tid; idx < nrows * nx; idx += T) {
+                const int r = fdiv(idx, p.mX), i = idx - r * nx;
+                stg_stream(out + (long long)r * p.out_dist + i, store_out(p, buf[r * p.PC + i]));
+            }
+        } else {
+            for (int idx = tid; idx < nrows * nx; idx += T) {
+                const int r = fdiv(idx, p.mX), i = idx - r * nx;
+                user_st(p, t0 + r, i, store_out(p, buf[r * p.PC + i]));
+            }
         }
         return;
     }
@@ -494,7 +546,7 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
     if (p.conv == CONV_RADER) {
         for (int idx = tid; idx < nrows * nx; idx += T) {
             const int r = fdiv(idx, p.mX), i = idx - r * nx;
-            xs[r * p.XP + i] = load_in(p, ldg_stream(in + (long long)r * p.in_dist + i));
+            xs[r * p.XP + i] = load_in(p, user_ld<V>(p, t0 + r, i));
         }
         __syncthreads();
         const int L = nx - 1;
@@ -507,7 +559,7 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
             const int r = fdiv(idx, p.mM), j = idx - r * M;
             V v = zero<V>();
             if (j < nx) {
-                V x = load_in(p, ldg_stream(in + (long long)r * p.in_dist + j));
+                V x = load_in(p, user_ld<V>(p, t0 + r, j));
                 v = fromd<V>(cmul(tod(x), __ldg(p.chirp + j)));
             }
             buf[r * p.PC + j] = v;
@@ -555,14 +607,14 @@ __device__ __forceinline__ void rows_body(const KParams& p, unsigned char* smem)
         __syncthreads();
         for (int idx = tid; idx < nrows * nx; idx += T) {
             const int r = fdiv(idx, p.mX), i = idx - r * nx;
-            stg_stream(out + (long long)r * p.out_dist + i, store_out(p, xs[r * p.XP + i]));
+            user_st(p, t0 + r, i, store_out(p, xs[r * p.XP + i]));
         }
     } else {
         for (int idx = tid; idx < nrows * nx; idx += T) {
             const int r = fdiv(idx, p.mX), k = idx - r * nx;
             const V c = conjv(buf[r * p.PC + k]);
             const V y = fromd<V>(cmul(tod(c), __ldg(p.chirp + k)));
-            stg_stream(out + (long long)r * p.out_dist + k, store_out(p, y));
+            user_st(p, t0 + r, k, store_out(p, y));
         }
     }
 }
@@ -787,20 +839,28 @@ __device__ __forceinline__ void four_twiddle_local(const KParams& p, V* buf, con
 template <typename V, class K>
 __device__ __forceinline__ void four_prefetch(const KParams& p, V* dst, int t, unsigned c) {
     const int T = blockDim.x, tid = opaque_tid();
-    const V* in = (const V*)p.in + (long long)t * p.in_dist;
     if (p.conv == CONV_RADER) {
         const int XC = p.XP;                      // staging of this CTA's x chunk
         for (int i = tid; i < XC; i += T) {
             const int gi = c * XC + i;
-            if (gi < p.nx) cp_async_elem(dst + i, in + gi);
+            if (gi < p.nx) user_cp(p, dst + i, t, gi);
         }
     } else {
         const int N2 = K::N2(p), W = K::W(p), PA = K::PA(p), total = K::N1(p) * W;
         const int lim = (p.conv == CONV_BLUE) ? p.nx : 0x7fffffff;
-        for (int idx = tid; idx < total; idx += T) {
-            const int i1 = K::dW(p, idx), j = idx - i1 * W;
-            const int jj = i1 * N2 + c * W + j;
-            if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
+        if (p.in_fmt == IO_PLAIN) {
+            const V* in = (const V*)p.in + (long long)t * p.in_dist;
+            for (int idx = tid; idx < total; idx += T) {
+                const int i1 = K::dW(p, idx), j = idx - i1 * W;
+                const int jj = i1 * N2 + c * W + j;
+                if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
+            }
+        } else {
+            for (int idx = tid; idx < total; idx += T) {
+                const int i1 = K::dW(p, idx), j = idx - i1 * W;
+                const int jj = i1 * N2 + c * W + j;
+                if (jj < lim) dst[i1 * PA + j] = user_ld<V>(p, t, jj);
+            }
         }
     }
     cp_async_commit();
@@ -820,7 +880,6 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     const int T = blockDim.x, tid = opaque_tid();
     const int N1 = K::N1(p), N2 = K::N2(p), W = K::W(p), R1 = K::R1(p), nx = p.nx;
     const int PA = K::PA(p), PC = K::PC(p);
-    V* out = (V*)p.out + (long long)t * p.out_dist;
     cp_async_wait_all();
     __syncthreads();
 
@@ -896,11 +955,18 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
 
     if (p.conv == CONV_NONE) {
         // X[k1 + N1 k2] from row layout (r, k2), k1 = c*R1 + r
+        if (p.out_fmt == IO_PLAIN) {
+            V* out = (V*)p.out + (long long)t * p.out_dist;
 #pragma unroll 4
-        for (int idx = tid; idx < R1 * N2; idx += T) {
-            const int k2 = K::dR1(p, idx), r = idx - k2 * R1;
-            stg_stream(out + (long long)(c * R1 + r) + (long long)N1 * k2,
-                       store_out(p, bufC[r * PC + k2]));
+            for (int idx = tid; idx < R1 * N2; idx += T) {
+                const int k2 = K::dR1(p, idx), r = idx - k2 * R1;
+                stg_stream(out + (long long)(c * R1 + r) + (long long)N1 * k2, store_out(p, bufC[r * PC + k2]));
+            }
+        } else {
+            for (int idx = tid; idx < R1 * N2; idx += T) {
+                const int k2 = K::dR1(p, idx), r = idx - k2 * R1;
+                user_st(p, t, (long long)(c * R1 + r) + (long long)N1 * k2, store_out(p, bufC[r * PC + k2]));
+            }
         }
         return;
     }
@@ -930,7 +996,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
             const int jj = j1 * N2 + c * W + j;
             if (jj < nx) {
                 const V cv = conjv(buf[j1 * PA + j]);
-                stg_stream(out + jj, store_out(p, fromd<V>(cmul(tod(cv), __ldg(p.chirp + jj)))));
+                user_st(p, t, jj, store_out(p, fromd<V>(cmul(tod(cv), __ldg(p.chirp + jj)))));
             }
         }
         return;
@@ -962,7 +1028,7 @@ __device__ __forceinline__ void four_transform(const KParams& p, V* buf, V* bufC
     __syncthreads();
     for (int i = tid; i < XC; i += T) {
         const int gi = c * XC + i;
-        if (gi < nx) stg_stream(out + gi, store_out(p, xs[i]));
+        if (gi < nx) user_st(p, t, gi, store_out(p, xs[i]));
     }
     // xs is rewritten by the next transform's prologue only after a
     // cluster barrier, so no extra barrier is needed here
@@ -1022,13 +1088,21 @@ template <typename V>
 __device__ __forceinline__ void colpass_issue(const KParams& p, int tile, V* dst) {
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
-    const V* in = (const V*)p.in + (long long)t * p.in_dist;
     const int N2 = p.N2, Vw = p.V, PA = p.PA, total = p.N1 * Vw;
     const long long lim = (p.pre == PRE_CHIRP) ? (long long)p.nx : (1LL << 62);
-    for (int idx = tid; idx < total; idx += T) {
-        const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
-        const long long jj = (long long)i1 * N2 + c0 + j;
-        if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
+    if (p.in_fmt == IO_PLAIN) {
+        const V* in = (const V*)p.in + (long long)t * p.in_dist;
+        for (int idx = tid; idx < total; idx += T) {
+            const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
+            const long long jj = (long long)i1 * N2 + c0 + j;
+            if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
+        }
+    } else {
+        for (int idx = tid; idx < total; idx += T) {
+            const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
+            const long long jj = (long long)i1 * N2 + c0 + j;
+            if (jj < lim) dst[i1 * PA + j] = user_ld<V>(p, t, jj);
+        }
     }
 }
 // prologue on the arrived tile; returns whether it wrote (caller syncs)
@@ -1099,14 +1173,27 @@ __device__ __forceinline__ void rowpass_finish(const KParams& p, int tile, V* bu
     V* out = (V*)p.out + (long long)t * p.out_dist;
     const int N1 = p.N1, N2 = p.N2, Vw = p.V, PC = p.PC;
     run_subffts<V, EMAX, 2>(buf, p.pc, tw, Vw, 1, PC);
+    if (p.out_fmt != IO_PLAIN) {
+        // the caller's strided or ComplexF16 layout (the last stage of a fused plan)
+        for (int idx = tid; idx < Vw * N2; idx += T) {
+            const int k2 = fdiv(idx, p.mV), r = idx - k2 * Vw;
+            const long long k = (long long)(r0 + r) + (long long)N1 * k2;
+            const V v = buf[r * PC + k2];
+            if (p.post == POST_CHIRP) {
+                if (k < p.nx) user_st(p, t, k, store_out(p, fromd<V>(cmul(tod(conjv(v)), __ldg(p.chirp + k)))));
+            } else {
+                user_st(p, t, k, store_out(p, v));
+            }
+        }
+        return;
+    }
 #pragma unroll 4
     for (int idx = tid; idx < Vw * N2; idx += T) {
         const int k2 = fdiv(idx, p.mV), r = idx - k2 * Vw;
         const long long k = (long long)(r0 + r) + (long long)N1 * k2;
         V v = buf[r * PC + k2];
         if (p.post == POST_CHIRP) {
-            if (k < p.nx)
-                stg_stream(out + k, store_out(p, fromd<V>(cmul(tod(conjv(v)), __ldg(p.chirp + k)))));
+            if (k < p.nx) stg_stream(out + k, store_out(p, fromd<V>(cmul(tod(conjv(v)), __ldg(p.chirp + k)))));
         } else if (p.post == POST_RAW) {
             out[k] = v;                       // intermediate of a convolution
         } else {

@@ -65,13 +65,21 @@ struct KParams {
     unsigned long long mW, mN2, mR1, mX, mM, mL, mV;
     int blk0;                     // first block of this parameter block in its launch
     unsigned char in_user, out_user;  // batched launches: in/out relative to the caller's buffers
-    unsigned char pad_[2];
+    unsigned char in_fmt, out_fmt;    // IO_*: how in / out hold the caller's elements
     long long in_off, out_off;    // batched launches: element offsets added to the bases
     // power-of-two passes: the four-step table of w_n (row pass) and the
     // single-level table w_N1^e, e < N1 (column pass)
     TwoLevel t4n;
     const double2* twN1;
+    // element strides of in / out (IO_STRIDED, IO_HALF; unused for IO_PLAIN)
+    long long in_stride, out_stride;
 };
+// The caller's buffers as a plan's first and last stage address them:
+// contiguous elements of the data type (IO_PLAIN), elements of the data type
+// at a stride (IO_STRIDED), or ComplexF16 elements at a stride (IO_HALF, the
+// arithmetic in ComplexF32).  Element i of transform t sits at
+// t * dist + i * stride.
+enum { IO_PLAIN = 0, IO_STRIDED = 1, IO_HALF = 2 };
 
 // COLPASS / ROWPASS stage their sub-transform twiddle table in shared memory
 // (ahead of the tile) when it is small; larger tables are read from L2.

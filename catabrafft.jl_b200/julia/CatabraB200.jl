@@ -114,9 +114,33 @@ export_wisdom(path::AbstractString) = check(ccall((:cfft_wisdom_export, LIB), Ci
 import_wisdom(path::AbstractString) = check(ccall((:cfft_wisdom_import, LIB), Cint, (Cstring,), path))
 forget_wisdom() = check(ccall((:cfft_wisdom_forget, LIB), Cint, ()))
 
-# the device fault word: 0 unless a kernel's bounded wait on its tensor
-# copies gave up (that launch's results are then incomplete)
+# the device fault word: 0 unless a kernel's bounded wait gave up (bit 0: a
+# tensor copy, bit 1: a work-queue or dataflow dependency); that launch's
+# results are then incomplete
 device_faults(clear::Bool = false) = ccall((:cfft_device_faults, LIB), Cint, (Cint,), clear ? 1 : 0)
+
+# batched form: many transforms of mixed lengths packed back to back in one
+# device buffer (pointers from CUDA.jl, e.g. `pointer(x)` of a CuVector),
+# one graph launch of the work-queue kernel per execution
+const BATCH_GROUPED = Cint(32)
+mutable struct Batch
+    lengths::Vector{Int64}
+    handle::Ptr{Cvoid}
+    function Batch(lengths::Vector{Int64}, ::Type{T}; grouped::Bool = false) where {T<:Union{Float32,Float64}}
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:cfft_batch_create, LIB), Cint, (Ref{Ptr{Cvoid}}, Int64, Ptr{Int64}, Cint, Cint),
+                    h, length(lengths), lengths, dtype_code(T), grouped ? BATCH_GROUPED : Cint(0)))
+        b = new(copy(lengths), h[])
+        finalizer(b) do b
+            b.handle == C_NULL || ccall((:cfft_batch_destroy, LIB), Cint, (Ptr{Cvoid},), b.handle)
+            b.handle = C_NULL
+        end
+        return b
+    end
+end
+execute!(b::Batch, d_out::Ptr{Cvoid}, d_in::Ptr{Cvoid}, dir::Cint = CFFT_FORWARD, stream::Ptr{Cvoid} = C_NULL) =
+    check(ccall((:cfft_batch_execute, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Ptr{Cvoid}),
+                b.handle, d_in, d_out, dir, stream))
 
 function empty_cache()
     for p in values(PLANS)
