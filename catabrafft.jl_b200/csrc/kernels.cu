@@ -333,6 +333,40 @@ cudaError_t cfft_launch_p2row_tma2(const void* f, const KParams& p, unsigned gri
     if (e != cudaSuccess) cudaGetLastError();
     return e;
 }
+cudaError_t cfft_launch_mixc_tma(const void* f, const KParams& p, unsigned grid, int threads, size_t smem,
+                                 int cluster, cudaStream_t st) {
+    auto enc = tensor_map_encoder();
+    if (!f || !enc) return cudaErrorNotSupported;
+    const int C = p.C, L = p.N2;
+    const int B = mix_box_rows(L);
+    if (C < 1 || L < 1 || p.batch < 1 || ((uintptr_t)p.in & 15)) return cudaErrorInvalidValue;
+    CUtensorMap tm;
+    const cuuint64_t dims[3] = {(cuuint64_t)(2 * C), (cuuint64_t)L, (cuuint64_t)p.batch};
+    const cuuint64_t strides[2] = {(cuuint64_t)C * 16, (cuuint64_t)p.in_dist * 16};
+    const cuuint32_t box[3] = {2, (cuuint32_t)B, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)p.in, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    KParams pc = p;
+    void* args[] = {(void*)&tm, (void*)&pc};
+    cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
 // The timeout path of the bounded waits, exercised without a fault: one
 // thread arms nothing and waits on a fresh mbarrier's phase 0, which no one
 // completes; after `polls` polls the wait gives up and records the fault bit
@@ -406,9 +440,15 @@ __global__ void __launch_bounds__(S::T, MB) k_mixc(KParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     mixc_body<V, S, GTAB>(p, smem);
 }
+// ComplexF64 with the strided input by tensor copies (tm: see mixc_body)
+template <class S, int MB>
+__global__ void __launch_bounds__(S::T, MB) k_mixc_tma(const __grid_constant__ CUtensorMap tm, KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    mixc_body<double2, S, false, true>(p, smem, &tm);
+}
 struct MixEntry {
     int n, C, L, threads;
-    const void* fn[2];            // ComplexF64, ComplexF32
+    const void* fn[2];            // ComplexF64, ComplexF32 (nullptr: none)
 };
 // 30240 = 7 x 4320, 4320 = 16 x 18 x 15 on 288 threads (variants 0, 1), and
 // 30240 = 9 x 3360, 3360 = 14 x 16 x 15 on 240 threads (variants 2 and 3:
@@ -416,16 +456,20 @@ struct MixEntry {
 // at most; three or two CTAs per SM)
 using Mix30240 = MixShape<7, 16, 18, 15, 288>;
 using Mix30240b = MixShape<9, 14, 16, 15, 240>;
-static const MixEntry kMix[][4] = {
+// variants 4 and 5: ComplexF64 by tensor copies, both splits, two CTAs per SM
+static const MixEntry kMix[][6] = {
     {{30240, 7, 4320, 288, {(const void*)k_mixc<double2, Mix30240, 2, false>, (const void*)k_mixc<float2, Mix30240, 2, false>}},
      {30240, 7, 4320, 288, {(const void*)k_mixc<double2, Mix30240, 3, true>, (const void*)k_mixc<float2, Mix30240, 3, true>}},
      {30240, 9, 3360, 240, {(const void*)k_mixc<double2, Mix30240b, 3, false>, (const void*)k_mixc<float2, Mix30240b, 3, false>}},
-     {30240, 9, 3360, 240, {(const void*)k_mixc<double2, Mix30240b, 2, false>, (const void*)k_mixc<float2, Mix30240b, 2, false>}}},
+     {30240, 9, 3360, 240, {(const void*)k_mixc<double2, Mix30240b, 2, false>, (const void*)k_mixc<float2, Mix30240b, 2, false>}},
+     {30240, 7, 4320, 288, {(const void*)k_mixc_tma<Mix30240, 2>, nullptr}},
+     {30240, 9, 3360, 240, {(const void*)k_mixc_tma<Mix30240b, 2>, nullptr}}},
 };
 int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads) {
     for (const auto& row : kMix) {
-        if (row[0].n != n || variant < 0 || variant > 3) continue;
+        if (row[0].n != n || variant < 0 || variant > 5) continue;
         const MixEntry& m = row[variant];
+        if (!m.fn[dtype == CFFT_DT_C128 ? 0 : 1]) return 0;
         *fn = m.fn[dtype == CFFT_DT_C128 ? 0 : 1];
         *C = m.C;
         *L = m.L;

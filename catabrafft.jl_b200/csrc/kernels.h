@@ -59,8 +59,13 @@ size_t cfft_convc_smem(size_t elem_bytes);
 // (mixc.cuh): 1 and the kernel, C, L and threads per CTA, else 0; variant 0
 // stages both twiddle tables (two CTAs per SM), variant 1 reads the w_n
 // table through L2 (three CTAs per SM), variants 2 and 3 are another split
-// of n at three and two CTAs per SM
+// of n at three and two CTAs per SM, variants 4 and 5 the two splits with
+// the input by tensor copies (ComplexF64 only)
 int cfft_mixc_lookup(long long n, int dtype, int variant, const void** fn, int* C, int* L, int* threads);
+// variants 4 and 5 (ComplexF64, the strided input by tensor copies) launch
+// through this (a cluster of `cluster` CTAs of `threads`; KParams C, N2 = L)
+cudaError_t cfft_launch_mixc_tma(const void* fn, const KParams& p, unsigned grid, int threads, size_t smem,
+                                 int cluster, cudaStream_t st);
 // launch a one-thread kernel whose bounded wait (at most `polls` polls) runs
 // out on an mbarrier no one completes, and wait for it
 cudaError_t cfft_wait_probe(int polls);

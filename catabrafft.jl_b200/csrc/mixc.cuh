@@ -73,13 +73,28 @@ __device__ __forceinline__ void mx_tw_row(V* v, const double2* lo, const double2
     }
 }
 
+// rows of one tensor copy of the strided input (TMA): the largest divisor of
+// L that a box dimension allows (at most 256)
+__host__ __device__ constexpr int mix_box_rows(int L) {
+    int r = 1;
+    for (int d = 1; d <= 256 && d <= L; d++)
+        if (L % d == 0) r = d;
+    return r;
+}
+
 // KParams: t4 = two-level table of w_L, t4n = two-level table of w_n (both
 // staged in shared memory after the buffer unless GTAB), in / out at
 // in_dist / out_dist, batch = transforms (one per cluster).
 // GTAB: the w_n table is read through L2 instead of being staged (frees
-// its shared memory for a third CTA per SM)
-template <typename V, class S, bool GTAB = false>
-__device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem) {
+// its shared memory for a third CTA per SM).
+// TMA (ComplexF64): the CTA's stride-C subsequence arrives as L / B tensor
+// copies of B rows x 16 bytes (tm maps the input as [transform][t < L][2 C
+// doubles]) completing on an mbarrier after the tables; per-element cp.async
+// of the strided input writes shared memory one sector at a time (measured:
+// as many wavefronts as all the FFT exchanges together).  A copy that times
+// out records the fault and the CTA still takes every cluster barrier.
+template <typename V, class S, bool GTAB = false, bool TMA = false>
+__device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem, const CUtensorMap* tm = nullptr) {
     cg::cluster_group cl = cg::this_cluster();
     const int c = (int)cl.block_rank();
     const int tr = block_id(p) / S::C;
@@ -91,15 +106,27 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
     const int mlo = 1 << bn, mhi = (p.t4n.N + mlo - 1) / mlo + 1;
     double2 *llo = tab, *lhi = tab + nlo;
     const double2 *glo = GTAB ? p.t4n.lo : lhi + nhi, *ghi = GTAB ? p.t4n.hi : lhi + nhi + mlo;
+    uint64_t* bar = (uint64_t*)(tab + nlo + nhi + (GTAB ? 0 : mlo + mhi));
+    if constexpr (TMA) {
+        // slot t = x[c + C t]: box k covers t in [B k, B k + B)
+        constexpr int B = mix_box_rows(S::L);
+        if (opaque_tid() == 0) mbar_init(bar, 1);
+        __syncthreads();                        // the barrier is initialised before anyone waits
+        if (opaque_tid() == 0) {
+            mbar_expect_tx(bar, (unsigned)(S::L * sizeof(V)));
+#pragma unroll 1
+            for (int k = 0; k < S::L / B; k++) tma_load_3d(buf + B * k, tm, bar, 2 * c, B * k, tr);
+        }
+    }
     {
         // stage-0 inputs: thread b < NB0 owns slots b + NB0 m = x[c + C (b + NB0 m)]
         const int b = opaque_tid();
-        if (b < S::NB0) {
+        if (!TMA && b < S::NB0) {
             const V* x = (const V*)p.in + (long long)tr * p.in_dist + c + (long long)S::C * b;
 #pragma unroll
             for (int m = 0; m < S::R0; m++) cp_async_elem(buf + b + S::NB0 * m, x + (long long)S::C * S::NB0 * m);
         }
-        cp_async_commit();
+        if (!TMA) cp_async_commit();
         for (int i = b; i < nlo + nhi; i += S::T) tab[i] = (i < nlo) ? p.t4.lo[i] : p.t4.hi[i - nlo];
         if (!GTAB) {
             double2* gs = lhi + nhi;
@@ -110,7 +137,11 @@ __device__ __forceinline__ void mixc_body(const KParams& p, unsigned char* smem)
     {
         // stage 0: DFT_R0 over m, twiddle w_L^(b k), back into the same slots
         const int b = opaque_tid();
-        cp_async_wait_all();
+        if constexpr (TMA) {
+            if (!mbar_wait(bar, 0) && b == 0) record_fault(kFaultTmaTimeout);
+        } else {
+            cp_async_wait_all();
+        }
         if (b < S::NB0) {
 #pragma unroll
             for (int m = 0; m < S::R0; m++) v[m] = load_in(p, buf[b + S::NB0 * m]);

@@ -272,7 +272,8 @@ struct Stage {
     int max_units = 0;       // persistent kernels: co-resident clusters (0 = one per unit)
     size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
     unsigned persist = 0;    // kernels that loop over the batch: CTAs to launch at most
-    int launch = 0;          // 1 / 3: pass A by tensor copies (ComplexF64 / ComplexF32 pairs); 2: dataflow launch
+    int launch = 0;          // 1 / 3: pass A by tensor copies (ComplexF64 / ComplexF32 pairs); 2: dataflow
+                             // launch; 4: mixed-radix cluster kernel with tensor copies
     KParams kp2;             // dataflow launch: the pass-B parameters
     int flow_lag = 0, flow_depth = 0;
 };
@@ -588,15 +589,20 @@ static void convc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
 // mixed-radix lengths with a cluster kernel of register L-point CTAs
 // (mixc.cuh): n = C x L
 static void mixc_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
-    // measured on B200 (1024 x 30240): ComplexF64 0.594 ms with both tables
-    // staged at two CTAs per SM against 0.635 at three (which spills);
-    // ComplexF32 0.367 ms at three against 0.456 at two
-    const bool three_first = dtype != CFFT_C128;
-    for (int i = 0; i < 4; i++) {
-        const int var = i >= 2 ? i : (three_first ? 1 - i : i);
+    // measured on B200 (1024 x 30240, ComplexF64): the strided input by
+    // tensor copies 0.422 ms (9 x 3360, variant 5) and 0.447 ms (7 x 4320,
+    // variant 4) against 0.471 / 0.477 ms by cp.async at two CTAs per SM and
+    // 0.499 / 0.547 at three; ComplexF32 (no tensor copies: its 8-byte
+    // elements are below a box row) 0.464 ms at three CTAs per SM (variant
+    // 1) against 0.586 at two
+    static const int order128[] = {5, 4, 3, 0, 2, 1}, order64[] = {1, 0, 2, 3};
+    const int* order = dtype == CFFT_C128 ? order128 : order64;
+    const int count = dtype == CFFT_C128 ? 6 : 4;
+    for (int i = 0; i < count; i++) {
+        const int var = order[i];
         const void* fn = nullptr;
         int C = 0, L = 0, T = 0;
-        if (!cfft_mixc_lookup(n, dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, var, &fn, &C, &L, &T)) return;
+        if (!cfft_mixc_lookup(n, dtype == CFFT_C128 ? CFFT_DT_C128 : CFFT_DT_C64, var, &fn, &C, &L, &T)) continue;
         Shape s;
         s.mode = MODE_MIXC;
         s.conv = CONV_NONE;
@@ -670,7 +676,8 @@ static std::string shape_desc(const Shape& s, int64_t n) {
         return "pow2cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_MIXC)
         return "cluster(C=" + std::to_string(s.C) + ",L=" + std::to_string(s.N2) + " per CTA,threads=" +
-               std::to_string(s.V) + (s.var == 1 || s.var == 2 ? ",ctas_per_sm=3" : "") + ")";
+               std::to_string(s.V) + (s.var == 1 || s.var == 2 ? ",ctas_per_sm=3" : "") + (s.var >= 4 ? ",tma" : "") +
+               ")";
     if (s.mode == MODE_CONVC)
         return pre + "cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
     if (s.mode == MODE_P2COL)
@@ -1063,7 +1070,9 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.kp = kp;
         s.threads = T;
         s.smem = (((size_t)L * e + 15) & ~(size_t)15) +
-                 (size_t)(nlo + nhi + (sh.var == 1 ? 0 : mlo + mhi)) * sizeof(double2);
+                 (size_t)(nlo + nhi + (sh.var == 1 ? 0 : mlo + mhi)) * sizeof(double2) +
+                 (sh.var >= 4 ? 16 : 0);      // the tensor copies' mbarrier
+        s.launch = sh.var >= 4 ? 4 : 0;
         s.cluster = C;
         s.grid = 0;
         s.in_sel = 0;
@@ -1549,6 +1558,8 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
                 ce = cfft_launch_p2row_tma(s.fn, kp, grid, s.smem, st);
             } else if (s.launch == 3) {
                 ce = cfft_launch_p2row_tma2(s.fn, kp, grid, s.smem, st);
+            } else if (s.launch == 4) {
+                ce = cfft_launch_mixc_tma(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             } else {
                 ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             }

@@ -84,14 +84,14 @@ def test_bench_configuration_rows_vs_oracle(cb, n):
     """The benchmarked configuration itself: 1024 transforms of n = 30240
     (mixed radix) or n = 10007 (Rader), forward and inverse, rows 0, 511 and
     1023 against the oracle; the plans are the benchmark's: a cluster of
-    seven register 4320-point CTAs for 30240, a cluster of five register
-    4096-point CTAs for 10007's convolution."""
+    nine register 3360-point CTAs (input by tensor copies) for 30240, a
+    cluster of five register 4096-point CTAs for 10007's convolution."""
     import torch
     batch = 1024
     x = _device_batch(torch, n, batch, np.complex128, seed=n)
     with _CPlan(cb, n, batch, cb.C128) as p:
         desc = p.describe()
-        assert ("cluster(C=7,L=4320" in desc) == (n == 30240), desc
+        assert ("cluster(C=9,L=3360 per CTA,threads=240,tma)" in desc) == (n == 30240), desc
         assert ("rader(n=10007,M=20480)+cluster(C=5" in desc) == (n == 10007), desc
         y = _execute(cb, p.h, x, cb.FORWARD)
         z = _execute(cb, p.h, x, cb.INVERSE)
@@ -334,6 +334,26 @@ def test_pow2_dataflow_single_launch(cb, tmp_path):
                     assert p.launches() == 1, (n, p.describe())
                 _pow2_check(cb, n, batch, dtype, f"pow2(N1={n // 4096},N2=4096,ctas_per_sm=2,dataflow)",
                             flags=cb.MEASURE)
+        finally:
+            cb.forget_wisdom()
+    assert cb._lib.LIB.cfft_device_faults(1) == 0
+
+
+def test_mixed_cluster_tensor_copy_variants(cb, tmp_path):
+    """The ComplexF64 mixed-radix cluster kernels that load each CTA's
+    stride-C subsequence by tensor copies (30240 as 7 x 4320 and as
+    9 x 3360), reached through wisdom entries for MEASURE plans: forward,
+    inverse, backward and in place against the oracle, with a batch that
+    gives several transforms per cluster slot; no copy timed out."""
+    cb._lib.LIB.cfft_device_faults(1)
+    for sig, tag in (("7 0 30240 7 4320 7 288 a c v4", "cluster(C=7,L=4320 per CTA,threads=288,tma)"),
+                     ("7 0 30240 9 3360 9 240 a c v5", "cluster(C=9,L=3360 per CTA,threads=240,tma)")):
+        path = tmp_path / "mix.txt"
+        path.write_text(f"catabra-b200-wisdom 1\n30240 70 {cb.C128} {cb.MEASURE} | {sig}\n")
+        cb.forget_wisdom()
+        cb.import_wisdom(str(path))
+        try:
+            _pow2_check(cb, 30240, 70, np.complex128, tag, flags=cb.MEASURE)
         finally:
             cb.forget_wisdom()
     assert cb._lib.LIB.cfft_device_faults(1) == 0
