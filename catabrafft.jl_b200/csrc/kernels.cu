@@ -204,6 +204,21 @@ __global__ void __launch_bounds__(CFFT_THREADS, MB) k_p2cl(KParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     p2cl_body<V, C>(p, smem);
 }
+// ComplexF64 with the stride-C subsequence by tensor copies (two CTAs per SM)
+template <int C>
+__global__ void __launch_bounds__(CFFT_THREADS, 2) k_p2cl_tma(const __grid_constant__ CUtensorMap tm, KParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    p2cl_body<double2, C, true>(p, smem, &tm);
+}
+const void* cfft_p2cl_tma_kernel(int C) {
+    switch (C) {
+        case 2: return (const void*)k_p2cl_tma<2>;
+        case 4: return (const void*)k_p2cl_tma<4>;
+        case 8: return (const void*)k_p2cl_tma<8>;
+        case 16: return (const void*)k_p2cl_tma<16>;
+    }
+    return nullptr;
+}
 template <typename V, int MB> static const void* p2cl_for(int C) {
     switch (C) {
         case 2: return (const void*)k_p2cl<V, 2, MB>;
@@ -333,17 +348,19 @@ cudaError_t cfft_launch_p2row_tma2(const void* f, const KParams& p, unsigned gri
     if (e != cudaSuccess) cudaGetLastError();
     return e;
 }
-cudaError_t cfft_launch_mixc_tma(const void* f, const KParams& p, unsigned grid, int threads, size_t smem,
-                                 int cluster, cudaStream_t st) {
+// a cluster kernel whose CTA c reads the stride-C subsequence x[c + C t],
+// t < L, of its transform by tensor copies of `rows` x 16 bytes: the map is
+// [transform][t < L][2 C doubles] (strides C x 16 B, in_dist x 16 B)
+static cudaError_t launch_subseq_tma(const void* f, const KParams& p, int C, int L, int rows, unsigned grid,
+                                     int threads, size_t smem, int cluster, cudaStream_t st) {
     auto enc = tensor_map_encoder();
     if (!f || !enc) return cudaErrorNotSupported;
-    const int C = p.C, L = p.N2;
-    const int B = mix_box_rows(L);
-    if (C < 1 || L < 1 || p.batch < 1 || ((uintptr_t)p.in & 15)) return cudaErrorInvalidValue;
+    if (C < 1 || L < 1 || rows < 1 || rows > 256 || L % rows || p.batch < 1 || ((uintptr_t)p.in & 15))
+        return cudaErrorInvalidValue;
     CUtensorMap tm;
     const cuuint64_t dims[3] = {(cuuint64_t)(2 * C), (cuuint64_t)L, (cuuint64_t)p.batch};
     const cuuint64_t strides[2] = {(cuuint64_t)C * 16, (cuuint64_t)p.in_dist * 16};
-    const cuuint32_t box[3] = {2, (cuuint32_t)B, 1};
+    const cuuint32_t box[3] = {2, (cuuint32_t)rows, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)p.in, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -366,6 +383,14 @@ cudaError_t cfft_launch_mixc_tma(const void* f, const KParams& p, unsigned grid,
     cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
     if (e != cudaSuccess) cudaGetLastError();
     return e;
+}
+cudaError_t cfft_launch_mixc_tma(const void* f, const KParams& p, unsigned grid, int threads, size_t smem,
+                                 int cluster, cudaStream_t st) {
+    return launch_subseq_tma(f, p, p.C, p.N2, mix_box_rows(p.N2), grid, threads, smem, cluster, st);
+}
+cudaError_t cfft_launch_p2cl_tma(const void* f, const KParams& p, unsigned grid, size_t smem, int cluster,
+                                 cudaStream_t st) {
+    return launch_subseq_tma(f, p, p.C, 4096, 256, grid, CFFT_THREADS, smem, cluster, st);
 }
 // The timeout path of the bounded waits, exercised without a fault: one
 // thread arms nothing and waits on a fresh mbarrier's phase 0, which no one

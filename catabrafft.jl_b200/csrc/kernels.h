@@ -33,6 +33,11 @@ const void* cfft_p2col_kernel(int dtype, int N1, int mb);
 // register 4096-point CTAs, mb = 2 or 3 CTAs per SM; shared memory
 // cfft_r4096_smem
 const void* cfft_p2cl_kernel(int dtype, int C, int mb);
+// ComplexF64, the stride-C subsequences by tensor copies (two CTAs per SM),
+// and its launcher (cluster of C CTAs)
+const void* cfft_p2cl_tma_kernel(int C);
+cudaError_t cfft_launch_p2cl_tma(const void* fn, const KParams& p, unsigned grid, size_t smem, int cluster,
+                                 cudaStream_t st);
 // both power-of-two passes in one persistent dataflow launch (N1 = 8 ..
 // 1024): kernel, shared memory (staged_entries = w_n table entries staged,
 // or 0) and launcher; ctr (ticket, abort flag, 2 nb counters) must be zero,

@@ -273,7 +273,7 @@ struct Stage {
     size_t smem_batched = 0; // shared memory of the descriptor-driven variant (0: smem)
     unsigned persist = 0;    // kernels that loop over the batch: CTAs to launch at most
     int launch = 0;          // 1 / 3: pass A by tensor copies (ComplexF64 / ComplexF32 pairs); 2: dataflow
-                             // launch; 4: mixed-radix cluster kernel with tensor copies
+                             // launch; 4 / 5: mixed-radix / power-of-two cluster kernel with tensor copies
     KParams kp2;             // dataflow launch: the pass-B parameters
     int flow_lag = 0, flow_depth = 0;
 };
@@ -503,7 +503,13 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
     // against 0.92 / 0.93 ms), so there they follow the two-pass shapes
     std::vector<Shape> cl;
     if (n <= 65536) {
-        for (int mb : {2, 3}) {
+        // var 1: ComplexF64 with the subsequences by tensor copies (two CTAs
+        // per SM), offered last: measured slower than the direct strided
+        // loads into registers (8192: 0.747 against 0.573 ms per GiB; 16384:
+        // 0.757 against 0.698), which overlap better with the compute
+        for (int c = 0; c < 3; c++) {
+            const int var = c == 2 ? 1 : 0, mb = c == 1 ? 3 : 2;
+            if (var == 1 && dtype != CFFT_C128) continue;
             Shape s;
             s.mode = MODE_P2CL;
             s.conv = CONV_NONE;
@@ -512,6 +518,7 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
             s.N2 = 4096;
             s.C = (int)(n / 4096);
             s.V = mb;
+            s.var = var;
             s.rc = {16, 16, 16};
             cl.push_back(s);
         }
@@ -540,8 +547,11 @@ static void pow2_candidates(int64_t n, int dtype, std::vector<Shape>& out) {
         s.rc = {16, 16, 16};
         flow.push_back(s);
     }
+    // ComplexF64 pass A at two CTAs per SM first (no spills; measured on
+    // B200 with tensor copies: 2^15 0.819 against 0.881 ms per GiB at three,
+    // 2^16 0.830 against 0.919)
     for (int c = 0; c < 4; c++) {
-        const int var = ((c < 2) == tma_first) ? 1 : 0, mb = (c % 2 == 0) ? 3 : 2;
+        const int var = ((c < 2) == tma_first) ? 1 : 0, mb = (c % 2 == 0) ? 2 : 3;
         // ComplexF32: pass A by cp.async at three CTAs per SM, or by tensor
         // copies of subsequence pairs at two
         if (dtype != CFFT_C128 && mb != (var == 1 ? 2 : 3)) continue;
@@ -673,7 +683,8 @@ static std::string shape_desc(const Shape& s, int64_t n) {
     if (s.mode == MODE_ROWS)
         return pre + "rows(V=" + std::to_string(s.V) + ")[" + join(s.rc) + "]";
     if (s.mode == MODE_P2CL)
-        return "pow2cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) + ")";
+        return "pow2cluster(C=" + std::to_string(s.C) + ",4096 per CTA,ctas_per_sm=" + std::to_string(s.V) +
+               (s.var == 1 ? ",tma" : "") + ")";
     if (s.mode == MODE_MIXC)
         return "cluster(C=" + std::to_string(s.C) + ",L=" + std::to_string(s.N2) + " per CTA,threads=" +
                std::to_string(s.V) + (s.var == 1 || s.var == 2 ? ",ctas_per_sm=3" : "") + (s.var >= 4 ? ",tma" : "") +
@@ -1036,7 +1047,8 @@ static int plan_build(cfft_plan_s* P, const Shape& sh) {
         s.grid = 0;
         s.in_sel = 0;
         s.out_sel = 1;
-        s.fn = cfft_p2cl_kernel(P->dtype, sh.C, sh.V);
+        s.fn = sh.var == 1 ? cfft_p2cl_tma_kernel(sh.C) : cfft_p2cl_kernel(P->dtype, sh.C, sh.V);
+        s.launch = sh.var == 1 ? 5 : 0;
         if (!s.fn) return fail(CFFT_ERR_UNSUPPORTED, "no power-of-two cluster kernel for C=" + std::to_string(sh.C));
         CUDA_TRY(cfft_prepare_fn(s.fn, s.smem, sh.C));
         int nclusters = 0;
@@ -1560,6 +1572,8 @@ static int plan_execute(cfft_plan_s* P, const void* in, void* out, int dir, cuda
                 ce = cfft_launch_p2row_tma2(s.fn, kp, grid, s.smem, st);
             } else if (s.launch == 4) {
                 ce = cfft_launch_mixc_tma(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
+            } else if (s.launch == 5) {
+                ce = cfft_launch_p2cl_tma(s.fn, kp, grid, s.smem, s.cluster, st);
             } else {
                 ce = cfft_launch_fn(s.fn, kp, grid, s.threads, s.smem, s.cluster, st);
             }

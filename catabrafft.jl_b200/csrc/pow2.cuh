@@ -349,8 +349,8 @@ __device__ __forceinline__ void p2col_body(const KParams& p, unsigned char* smem
 // data crosses HBM once (the two-pass form writes and reads an
 // intermediate).  KParams: t4 = two-level table of w_4096 (staged), t4n =
 // two-level table of w_n (read through L2), batch = transforms.
-template <typename V, int C>
-__device__ __forceinline__ void p2cl_body(const KParams& p, unsigned char* smem) {
+template <typename V, int C, bool TMA = false>
+__device__ __forceinline__ void p2cl_body(const KParams& p, unsigned char* smem, const CUtensorMap* tm = nullptr) {
     cg::cluster_group cl = cg::this_cluster();
     const int c = (int)cl.block_rank();
     const int tr = block_id(p) / C;
@@ -359,15 +359,36 @@ __device__ __forceinline__ void p2cl_body(const KParams& p, unsigned char* smem)
     double2* tlo = after16(buf + 16 * R4096_PL);
     double2* thi = tlo + 64;
     V v[16];
-    {
+    if constexpr (TMA) {
+        // ComplexF64: the stride-C subsequence by 16 tensor copies of 256
+        // elements (tm maps the input as [transform][t < 4096][2 C doubles])
+        // into buf[t], each thread then reading its own slots t + 256 k,
+        // which the first exchange overwrites only from the same thread
+        uint64_t* bar = (uint64_t*)(thi + 65);
+        const int t = opaque_tid();
+        if (t == 0) mbar_init(bar, 1);
+        if (t < 64) tlo[t ^ (t >> 3)] = p.t4.lo[t];
+        if (t < 65) thi[t] = p.t4.hi[t];
+        __syncthreads();                        // barrier initialised, tables staged
+        if (t == 0) {
+            mbar_expect_tx(bar, 4096 * (unsigned)sizeof(V));
+#pragma unroll 1
+            for (int k = 0; k < 16; k++) tma_load_3d(buf + 256 * k, tm, bar, 2 * c, 256 * k, tr);
+        }
+        // a copy that timed out records the fault; the CTA still takes the
+        // cluster barrier below
+        if (!mbar_wait(bar, 0) && t == 0) record_fault(kFaultTmaTimeout);
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] = load_in(p, buf[t + 256 * k]);
+    } else {
         const int t = opaque_tid();
         if (t < 64) tlo[t ^ (t >> 3)] = p.t4.lo[t];
         if (t < 65) thi[t] = p.t4.hi[t];
         const V* x = (const V*)p.in + (long long)tr * p.in_dist + c + (long long)C * t;
 #pragma unroll
         for (int k = 0; k < 16; k++) v[k] = load_in(p, __ldg(x + (long long)C * 256 * k));
+        __syncthreads();                        // tables staged
     }
-    __syncthreads();                            // tables staged
     fft4096_regs(v, buf, tlo, thi, opaque_tid());
     {
         const int t = opaque_tid();

@@ -77,7 +77,7 @@ def test_python_api_argument_errors():
     (1, "rows"), (4096, "rows(V=1)[16,16,16]"), (30240, "cluster(C=9,L=3360 per CTA,threads=240,tma)"), (10007, "rader(n=10007,M=20480)+cluster(C=5"),
     (89, "rader(n=89,M=175)+rows"), (10006, "bluestein(n=10006,M=20160)"),
     (2 ** 20, "pow2(N1=256,N2=4096"), (2 ** 22, "pow2(N1=1024,N2=4096"), (2 ** 23, "twopass(N1=2048,N2=4096)"),
-    (2 ** 15, "pow2(N1=8,N2=4096,ctas_per_sm=3,tma)"), (2 ** 14, "pow2cluster(C=4,4096 per CTA,ctas_per_sm=2)"), (60480, "four(C="),
+    (2 ** 15, "pow2(N1=8,N2=4096,ctas_per_sm=2,tma)"), (2 ** 14, "pow2cluster(C=4,4096 per CTA,ctas_per_sm=2)"), (60480, "four(C="),
 ])
 def test_strategy_choice(n, expect):
     m = load()

@@ -214,7 +214,7 @@ def test_pow2_register_passes(cb, dtype):
         if n <= 16384:                              # one pass on a cluster of N1 CTAs
             _pow2_check(cb, n, batch, dtype, f"pow2cluster(C={N1},4096 per CTA,ctas_per_sm=2)")
         else:
-            shape = "ctas_per_sm=3,tma)" if dtype == np.complex128 else "ctas_per_sm=2,tma)"
+            shape = "ctas_per_sm=2,tma)"
             _pow2_check(cb, n, batch, dtype, f"pow2(N1={N1},N2=4096,{shape}")
     assert cb._lib.LIB.cfft_device_faults(1) == 0
 
@@ -356,4 +356,28 @@ def test_mixed_cluster_tensor_copy_variants(cb, tmp_path):
             _pow2_check(cb, 30240, 70, np.complex128, tag, flags=cb.MEASURE)
         finally:
             cb.forget_wisdom()
+    assert cb._lib.LIB.cfft_device_faults(1) == 0
+
+
+def test_pow2_cluster_tensor_copy_variant(cb, tmp_path):
+    """The ComplexF64 single-pass cluster kernel that loads each CTA's
+    stride-C subsequence by tensor copies (a timed candidate, slower than the
+    direct loads at 8192 and 16384), reached through wisdom entries for
+    MEASURE plans: every cluster size against the oracle, no copy timed out."""
+    cases = [(1 << 13, 300), (1 << 14, 150), (1 << 15, 80), (1 << 16, 40)]
+    cb._lib.LIB.cfft_device_faults(1)
+    lines = ["catabra-b200-wisdom 1"]
+    for n, batch in cases:
+        C = n // 4096
+        lines.append(f"{n} {batch} {cb.C128} {cb.MEASURE} | 8 0 {n} {C} 4096 {C} 2 a c 16 16 16 v1")
+    path = tmp_path / "p2cl_tma.txt"
+    path.write_text("\n".join(lines) + "\n")
+    cb.forget_wisdom()
+    cb.import_wisdom(str(path))
+    try:
+        for n, batch in cases:
+            _pow2_check(cb, n, batch, np.complex128, f"pow2cluster(C={n // 4096},4096 per CTA,ctas_per_sm=2,tma)",
+                        flags=cb.MEASURE)
+    finally:
+        cb.forget_wisdom()
     assert cb._lib.LIB.cfft_device_faults(1) == 0
