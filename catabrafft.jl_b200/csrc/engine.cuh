@@ -1135,15 +1135,17 @@ __device__ __forceinline__ void colpass_finish(const KParams& p, int tile, V* bu
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
     V* out = (V*)p.out + (long long)t * p.out_dist;
-    const int N1 = p.N1, N2 = p.N2, Vw = p.V, PA = p.PA, total = N1 * Vw;
+    const int N1 = p.N1, N2 = p.N2, Vw = p.V, PA = p.PA;
     run_subffts<V, EMAX, 2>(buf, p.pa, tw, Vw, PA, 1);
-    if (T % Vw == 0) {
-        // each thread keeps one column: no per-element division
-        // ... and forms its twiddles w^(c k1), k1 = k0, k0 + ks, ..., as FP64
-        // products with the step w^(c ks), re-seeded from the table every 16
-        // steps (the error stays near 1e-15; the same FP64 work per element
-        // as a table product, a sixteenth of its table reads)
-        const int j = tid % Vw, ks = T / Vw, k0 = tid / Vw;
+    // the first ks Vw threads (ks = T / Vw; all of them when Vw divides T)
+    // each keep one column: no per-element division, and the twiddles
+    // w^(c k1), k1 = k0, k0 + ks, ..., are FP64 products with the step
+    // w^(c ks), re-seeded from the table every 16 steps (the error stays near
+    // 1e-15; the same FP64 work per element as a table product, a sixteenth
+    // of its table reads)
+    const int ks = T / Vw;
+    if (tid < ks * Vw) {
+        const int j = tid % Vw, k0 = tid / Vw;
         const unsigned c = (unsigned)(c0 + j);
         V* o = out + c0 + j;
         const double2 st = tw_two(t4, c * (unsigned)ks);
@@ -1154,13 +1156,6 @@ __device__ __forceinline__ void colpass_finish(const KParams& p, int tile, V* bu
             if ((i & 15) == 0) w = tw_two(t4, c * (unsigned)k1);
             o[(long long)k1 * N2] = cmul(buf[k1 * PA + j], fromd<V>(w));
             w = cmul(w, st);
-        }
-    } else {
-#pragma unroll 4
-        for (int idx = tid; idx < total; idx += T) {
-            const int k1 = fdiv(idx, p.mV), j = idx - k1 * Vw;
-            const unsigned e = (unsigned)(c0 + j) * (unsigned)k1;
-            out[(long long)k1 * N2 + c0 + j] = apply_tw(buf[k1 * PA + j], t4, e);
         }
     }
 }
