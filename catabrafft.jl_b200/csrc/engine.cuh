@@ -1088,18 +1088,22 @@ template <typename V>
 __device__ __forceinline__ void colpass_issue(const KParams& p, int tile, V* dst) {
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
-    const int N2 = p.N2, Vw = p.V, PA = p.PA, total = p.N1 * Vw;
+    const int N1 = p.N1, N2 = p.N2, Vw = p.V, PA = p.PA;
     const long long lim = (p.pre == PRE_CHIRP) ? (long long)p.nx : (1LL << 62);
+    // the first ks Vw threads (ks = T / Vw) each take one column j of the
+    // tile, rows i1 = k0, k0 + ks, ...: no per-element division; a warp
+    // still reads runs of Vw consecutive elements of consecutive rows
+    const int ks = T / Vw;
+    if (tid >= ks * Vw) return;
+    const int j = tid % Vw, k0 = tid / Vw;
     if (p.in_fmt == IO_PLAIN) {
-        const V* in = (const V*)p.in + (long long)t * p.in_dist;
-        for (int idx = tid; idx < total; idx += T) {
-            const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
+        const V* in = (const V*)p.in + (long long)t * p.in_dist + c0 + j;
+        for (int i1 = k0; i1 < N1; i1 += ks) {
             const long long jj = (long long)i1 * N2 + c0 + j;
-            if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + jj);
+            if (jj < lim) cp_async_elem(dst + i1 * PA + j, in + (long long)i1 * N2);
         }
     } else {
-        for (int idx = tid; idx < total; idx += T) {
-            const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
+        for (int i1 = k0; i1 < N1; i1 += ks) {
             const long long jj = (long long)i1 * N2 + c0 + j;
             if (jj < lim) dst[i1 * PA + j] = user_ld<V>(p, t, jj);
         }
@@ -1111,10 +1115,13 @@ __device__ __forceinline__ bool colpass_fix(const KParams& p, int tile, V* buf) 
     if (p.pre == PRE_NONE && !p.dir) return false;
     const int T = blockDim.x, tid = opaque_tid();
     const int tiles = p.N2 / p.V, t = tile / tiles, c0 = (tile - t * tiles) * p.V;
-    const int N2 = p.N2, Vw = p.V, PA = p.PA, total = p.N1 * Vw;
+    const int N1 = p.N1, N2 = p.N2, Vw = p.V, PA = p.PA;
+    // one column per thread, as in colpass_issue (the caller synchronises)
+    const int ks = T / Vw;
+    if (tid >= ks * Vw) return true;
+    const int j = tid % Vw;
 #pragma unroll 4
-    for (int idx = tid; idx < total; idx += T) {
-        const int i1 = fdiv(idx, p.mV), j = idx - i1 * Vw;
+    for (int i1 = tid / Vw; i1 < N1; i1 += ks) {
         const long long jj = (long long)i1 * N2 + c0 + j;
         V* e = buf + i1 * PA + j;
         if (p.pre == PRE_NONE) {
@@ -1178,10 +1185,15 @@ __device__ __forceinline__ void rowpass_finish(const KParams& p, int tile, V* bu
     V* out = (V*)p.out + (long long)t * p.out_dist;
     const int N1 = p.N1, N2 = p.N2, Vw = p.V, PC = p.PC;
     run_subffts<V, EMAX, 2>(buf, p.pc, tw, Vw, 1, PC);
+    // the first ks Vw threads (ks = T / Vw) each store one row r of the
+    // tile, k2 = k0, k0 + ks, ...: no per-element division; a warp still
+    // writes runs of Vw consecutive outputs
+    const int ks = T / Vw;
+    if (tid >= ks * Vw) return;
+    const int r = tid % Vw, k0 = tid / Vw;
     if (p.out_fmt != IO_PLAIN) {
         // the caller's strided or ComplexF16 layout (the last stage of a fused plan)
-        for (int idx = tid; idx < Vw * N2; idx += T) {
-            const int k2 = fdiv(idx, p.mV), r = idx - k2 * Vw;
+        for (int k2 = k0; k2 < N2; k2 += ks) {
             const long long k = (long long)(r0 + r) + (long long)N1 * k2;
             const V v = buf[r * PC + k2];
             if (p.post == POST_CHIRP) {
@@ -1193,8 +1205,7 @@ __device__ __forceinline__ void rowpass_finish(const KParams& p, int tile, V* bu
         return;
     }
 #pragma unroll 4
-    for (int idx = tid; idx < Vw * N2; idx += T) {
-        const int k2 = fdiv(idx, p.mV), r = idx - k2 * Vw;
+    for (int k2 = k0; k2 < N2; k2 += ks) {
         const long long k = (long long)(r0 + r) + (long long)N1 * k2;
         V v = buf[r * PC + k2];
         if (p.post == POST_CHIRP) {
