@@ -166,6 +166,17 @@ template <typename V> __device__ __forceinline__ void user_cp(const KParams& p, 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// x / d for 0 <= x < 2^20 and 1 <= d < 2^20 (the block-level indices of the
+// radix passes): a fast single-precision quotient, within one of the true
+// quotient at these sizes (relative error ~2^-22 on operands exact in
+// float), truncated and then corrected by one integer step either way.
+__device__ __forceinline__ int udiv_small(int x, int d) {
+    int q = (int)__fdividef((float)x, (float)d);
+    const int r = x - q * d;
+    q += (r >= d) - (r < 0);
+    return q;
+}
+
 // ----------------------------------------------------- Stockham radix pass
 // One pass over Gw sub-transforms of length L held in smem: element i of
 // sub-transform g lives at buf[g*gs + i*is].  s = product of earlier radices.
@@ -180,15 +191,15 @@ __device__ __forceinline__ void spass(V* __restrict__ buf, int L, int Gw, int is
     constexpr int SL = EMAX / R;
     const int T = WARP ? 32 : (int)blockDim.x;
     const int tid = WARP ? (opaque_tid() & 31) : opaque_tid();
-    const int nb = L / R;
-    const int n1 = nb / s;            // butterflies per stride class = twiddle block width
+    const int nb = L / R;                  // R is a compile-time constant
+    const int n1 = udiv_small(nb, s);  // butterflies per stride class = twiddle block width
     const int W = Gw * nb;
     V v[SL][R];
     int off[SL], pp_[SL];
-    int g = tid % Gw, b = tid / Gw;
-    int pp = b / s, q = b - pp * s;
-    const int dg = T % Gw, db = T / Gw;
-    const int dpp = db / s, dq = db - dpp * s;
+    int b = udiv_small(tid, Gw), g = tid - b * Gw;
+    int pp = udiv_small(b, s), q = b - pp * s;
+    const int db = udiv_small(T, Gw), dg = T - db * Gw;
+    const int dpp = udiv_small(db, s), dq = db - dpp * s;
 #pragma unroll
     for (int i = 0; i < SL; i++) {
         const int w = tid + i * T;
